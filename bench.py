@@ -1,0 +1,403 @@
+"""Benchmark of the exact-decimal path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sweep|query]
+
+Workload "sweep" (default) is the precision sweep: element-wise a*b+c and a/b
+(scale s+4, half-up) on DECIMAL(p, p/4), p in {18,38,76,150,300,600}, every
+digit uniform 0-9, signs +/-, zero divisors redrawn, 16M rows for p<=38,
+halved per doubling of p.  One step = one pass over all twelve
+(p, expression) launches; inputs are resident in HBM and every case's input
+is larger than L2 (126 MB), so no L2 flush is needed between steps.
+
+Workload "query" is the grouped-aggregate query (4 DECIMAL(15,2) columns,
+two CHAR(1) keys, SUM x4 / AVG x3 / COUNT) at 256M rows.
+
+The reference arm (--impl reference) times the CPU restatement of the
+reference's decimal path (oracle/, the reference has no CPU decimal path of
+its own) on the host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+from ultraprecise_b200.workloads import SWEEP, sweep_expr  # noqa: E402
+METRIC = "decimal rows/s (precision sweep a*b+c and a/b, p=18..600), bit-exact"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "query"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# -------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max((float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, n in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------ workloads
+def limbs(nbytes: int) -> int:
+    return (nbytes + 3) // 4
+
+
+def sweep_cases(scale_rows: float = 1.0):
+    from ultraprecise_b200 import codec
+    cases = []
+    for p, rows in SWEEP:
+        s = p // 4
+        B = codec.compact_bytes(p)
+        for op in ("mad", "div"):
+            r = max(1, int(rows * scale_rows))
+            if op == "mad":
+                ob = codec.compact_bytes(2 * p + 1)
+                nin = 3
+                # limb multiply-adds per row: the a*b product plus aligning c by 10^s
+                la = limbs(B)
+                madds = la * la + la * limbs(max(1, ((10 ** s).bit_length() + 7) // 8))
+            else:
+                ob = codec.compact_bytes(max(s + 5, 1))
+                nin = 2
+                sh = s + 4
+                la = limbs(B)
+                nx = la + limbs(((10 ** sh).bit_length() + 7) // 8)
+                madds = la * limbs(((10 ** sh).bit_length() + 7) // 8) + (nx - la + 1) * la
+            cases.append({"p": p, "s": s, "op": op, "rows": r, "in_bytes": B, "n_in": nin, "out_bytes": ob,
+                          "bytes_per_row": nin * B + ob, "madds_per_row": madds})
+    return cases
+
+
+def build_expr(case):
+    return sweep_expr(case["p"], case["op"])
+
+
+# ---------------------------------------------------------- our arm
+def run_ours(args, rank, world):
+    import torch
+    from ultraprecise_b200 import abi, runtime
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = abi.load()
+    stream = torch.cuda.Stream()
+    cases = sweep_cases()
+    hbm_peak, peak_kind = peaks()
+    madd_peak = C.c_double(0)
+    abi.check(lib.up_util_imad_peak(C.byref(madd_peak), stream.cuda_stream), "imad peak")
+
+    mods, inputs, outs = [], [], []
+    with torch.cuda.stream(stream):
+        for i, c in enumerate(cases):
+            e, cols = build_expr(c)
+            m = runtime.compile_expr(e, cols)
+            mods.append(m)
+            ins = []
+            for k in range(c["n_in"]):
+                t = runtime.gen_digits(c["rows"], c["p"], seed=1_000_003 * (i + 1) + 7919 * k + rank,
+                                       nonzero=(c["op"] == "div" and k == 1), stream=stream)
+                ins.append(runtime.DeviceColumn(t, c["p"], c["s"]))
+            inputs.append(ins)
+            outs.append(torch.empty(c["rows"] * m.value_bytes, dtype=torch.uint8, device="cuda"))
+    torch.cuda.synchronize()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def step():
+        for i, (m, ins, o) in enumerate(zip(mods, inputs, outs)):
+            m.launch(ins, cases[i]["rows"], out=o, err=err, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    per_case = [0.0] * len(cases)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # per-kernel events on the launching stream, recorded inside the timed region
+    evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in cases]
+           for _ in range(args.steps)]
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for k in range(args.steps):
+            for i, (m, ins, o) in enumerate(zip(mods, inputs, outs)):
+                evs[k][i][0].record(stream)
+                m.launch(ins, cases[i]["rows"], out=o, err=err, stream=stream)
+                evs[k][i][1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    for k in range(args.steps):
+        for i in range(len(cases)):
+            per_case[i] += evs[k][i][0].elapsed_time(evs[k][i][1]) / args.steps
+    total_ms = max_over_ranks(total_ms, world)
+    rows_per_step = sum(c["rows"] for c in cases)
+    ms_per_step = total_ms / args.steps
+    value = rows_per_step * world / (ms_per_step * 1e-3)
+
+    case_rep = []
+    for c, ms in zip(cases, per_case):
+        gbs = c["bytes_per_row"] * c["rows"] / (ms * 1e-3) / 1e9
+        gmadds = c["madds_per_row"] * c["rows"] / (ms * 1e-3) / 1e9
+        case_rep.append({"p": c["p"], "op": c["op"], "rows": c["rows"], "ms": round(ms, 4),
+                         "rows_per_s": round(c["rows"] / (ms * 1e-3)),
+                         "hbm_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
+                         "int_gmadds": round(gmadds, 1), "int_frac": round(gmadds * 1e9 / madd_peak.value, 4)})
+    dom = max(range(len(cases)), key=lambda i: per_case[i])
+    dc, dr = cases[dom], case_rep[dom]
+    hbm_bound = dr["hbm_frac"] >= dr["int_frac"]
+    if hbm_bound:
+        roof = {"bound": "hbm", "achieved": dr["hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(dr["hbm_gbs"] / hbm_peak, 4), "traffic": None,
+                "kernel": f"up_expr_tile p={dc['p']} {dc['op']}", "peak_source": peak_kind}
+    else:
+        roof = {"bound": "int32", "achieved": dr["int_gmadds"], "peak": round(madd_peak.value / 1e9, 1),
+                "unit": "G limb-madd/s", "frac": dr["int_frac"], "traffic": None,
+                "kernel": f"up_expr_tile p={dc['p']} {dc['op']}",
+                "peak_source": "measured (up_util_imad_peak)",
+                "hbm_achieved_gbs": dr["hbm_gbs"], "hbm_frac": dr["hbm_frac"]}
+    res = {"metric": METRIC, "value": round(value), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+           "config": {"workload": "precision sweep (configs[1]): a*b+c and a/b on DECIMAL(p,p/4), "
+                                  "p in 18,38,76,150,300,600; 16M rows p<=38 halved per doubling",
+                      "rows_per_step_per_gpu": rows_per_step, "l2": "inputs larger than L2 (no flush)",
+                      "parallelism": f"replicas x{world} (row shards, no collective)"},
+           "roofline": roof, "cases": case_rep,
+           "gpu_launches": len(cases) * args.steps,
+           "imad_peak_gmadds": round(madd_peak.value / 1e9, 1)}
+    res["clocks"] = clk.summary()
+    if not args.no_e2e:
+        res["e2e"] = e2e_ours(args, cases, mods, world, stream)
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        res["cpu_baseline"] = cpu_baseline(cases, args.cpu_seconds)
+    return res
+
+
+def e2e_ours(args, cases, mods, world, stream):
+    """Same metric through the C ABI with HOST buffers: per step, every input
+    column is copied from pinned host memory, the kernel runs, and every
+    result is copied back to pinned host memory."""
+    import torch
+    from ultraprecise_b200 import runtime
+    host_in, host_out, dev_in, dev_out = [], [], [], []
+    for i, (c, m) in enumerate(zip(cases, mods)):
+        ins, dins = [], []
+        for k in range(c["n_in"]):
+            d = runtime.gen_digits(c["rows"], c["p"], seed=77 + 31 * i + k, nonzero=(c["op"] == "div" and k == 1))
+            h = torch.empty(d.numel(), dtype=torch.uint8, pin_memory=True)
+            h.copy_(d)
+            ins.append(h)
+            dins.append(torch.empty_like(d))
+        host_in.append(ins)
+        dev_in.append(dins)
+        host_out.append(torch.empty(c["rows"] * m.value_bytes, dtype=torch.uint8, pin_memory=True))
+        dev_out.append(torch.empty(c["rows"] * m.value_bytes, dtype=torch.uint8, device="cuda"))
+    h2d = sum(t.numel() for ins in host_in for t in ins)
+    d2h = sum(t.numel() for t in host_out)
+
+    def step():
+        with torch.cuda.stream(stream):
+            for i, (c, m) in enumerate(zip(cases, mods)):
+                cols = []
+                for k in range(c["n_in"]):
+                    dev_in[i][k].copy_(host_in[i][k], non_blocking=True)
+                    cols.append(runtime.DeviceColumn(dev_in[i][k], c["p"], c["s"]))
+                m.launch(cols, c["rows"], out=dev_out[i], stream=stream)
+                host_out[i].copy_(dev_out[i], non_blocking=True)
+
+    steps = max(1, min(args.steps, 3))
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(t0.elapsed_time(t1), world) / steps
+    rows = sum(c["rows"] for c in cases)
+    del dev_in, dev_out
+    return {"value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": steps}
+
+
+# ------------------------------------------------------ CPU baseline
+def cpu_rate(cases, cpu_seconds, threads, seed=1):
+    """Time the oracle on the host cores over the same sweep mix (every case
+    scaled by one common fraction of its rows), sized for ~cpu_seconds."""
+    from oracle import gen, oracle
+    from ultraprecise_b200 import codec
+    from ultraprecise_b200 import expr as E
+
+    def run(frac):
+        rows_tot, secs = 0, 0.0
+        for i, c in enumerate(cases):
+            r = max(8, int(c["rows"] * frac))
+            cols = [gen.compact_digits(r, c["p"], c["in_bytes"], seed + 31 * i + k,
+                                       nonzero=(c["op"] == "div" and k == 1)) for k in range(c["n_in"])]
+            e, ct = build_expr(c)
+            b = E.build([e], ct)
+            E.derive_types(b)
+            ob = codec.compact_bytes(b.nodes[b.roots[0]].precision)
+            t = time.perf_counter()
+            oracle.eval_expr(b, b.roots[0], cols, r, ob, threads=threads)
+            secs += time.perf_counter() - t
+            rows_tot += r
+        return rows_tot, secs
+
+    f0 = 1.0 / 65536
+    r0, s0 = run(f0)
+    frac = min(1.0 / 16, f0 * cpu_seconds / max(s0, 1e-4))
+    r1, s1 = run(frac)
+    return r1 / s1, frac, r1
+
+
+def cpu_baseline(cases, cpu_seconds):
+    threads = os.cpu_count() or 1
+    rate, frac, rows = cpu_rate(cases, cpu_seconds, threads)
+    return {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"{rows} rows: every sweep case at {frac:.2e} of its rows (same mix), oracle on "
+                      f"{threads} host threads"}
+
+
+# ---------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    """The reference's decimal arithmetic has no CPU implementation (it is
+    device-only PTX); its restatement in oracle/ runs on all host cores."""
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    cases = sweep_cases()
+    per = args.cpu_seconds / max(1, args.steps)
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_rate(cases, min(per, 2.0), threads, seed=99)
+    rates, rows = [], 0
+    for k in range(max(1, args.steps)):
+        r, frac, rows = cpu_rate(cases, per, threads, seed=1 + k)
+        rates.append(r)
+    rate = sorted(rates)[len(rates) // 2]
+    total_rows = sum(c["rows"] for c in cases)
+    return {"metric": METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_rows / rate * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "precision sweep (configs[1]) on host cores, bounded sample",
+                       "parallelism": f"{threads} host threads"},
+            "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
+                             "sample": f"{rows} rows per step: every sweep case at {frac:.2e} of its rows"},
+            "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---------------------------------------------------------- distributed
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_ours(args, rank, world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,51 @@
+/*
+ * ultraprecise_util.h — benchmark and test utilities of libultraprecise.so.
+ *
+ * These have no counterpart in the reference's decimal path: they produce the
+ * seeded synthetic columns that stand in for the reference's datasets (the
+ * TPC-H lineitem columns of its paper experiments and the data generators
+ * under append_expr_info/gen_data/, which are not shipped as data), flush the
+ * L2 cache between timed iterations, and measure the 32-bit integer
+ * multiply-add peak used as the roofline of the wide-precision kernels.
+ */
+#ifndef ULTRAPRECISE_UTIL_H_
+#define ULTRAPRECISE_UTIL_H_
+
+#include "ultraprecise.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Seeded random compact decimals of precision p written to `out` (DEVICE,
+ * rows * up_compact_bytes(p) bytes).  Every one of the p digits is uniform
+ * 0-9 (the precision-sweep distribution); signs are +/- with equal odds when
+ * signed_ != 0.  nonzero != 0 redraws an all-zero value (a zero divisor). */
+up_status up_util_gen_digits(void* out, int64_t rows, int32_t precision, uint64_t seed,
+                             int32_t signed_, int32_t nonzero, void* stream);
+
+/* Seeded random compact decimals whose unscaled integer is
+ * lo + step * U{0 .. (hi-lo)/step}; lo, hi, step must fit int64 and the value
+ * must fit the compact width of p. */
+up_status up_util_gen_range(void* out, int64_t rows, int32_t precision, int64_t lo, int64_t hi,
+                            int64_t step, uint64_t seed, void* stream);
+
+/* Write `bytes` of a scratch buffer (DEVICE) to evict L2. */
+up_status up_util_flush_l2(void* buf, int64_t bytes, void* stream);
+
+/* Measure the 32-bit integer multiply-add throughput of the current device:
+ * a dependent-free chain of 64-bit-accumulating multiply-adds (the operation
+ * the limb multiply loops issue).  Returns multiply-adds per second. */
+up_status up_util_imad_peak(double* madds_per_s, void* stream);
+
+/* Compile a kernel source with the library's NVRTC settings without loading
+ * it (no GPU needed).  Returns UP_OK or UP_ERR_COMPILE with the log in
+ * up_last_error_message(). */
+up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
+                               const up_col_type* cols, int32_t n_cols, int32_t query,
+                               const up_query_agg* aggs, int32_t n_aggs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

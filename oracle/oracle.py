@@ -1,0 +1,120 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU baseline / reference arm.  Never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+from ultraprecise_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        build()
+    lib = C.CDLL(LIB)
+    P = C.c_void_p
+    lib.orc_compact_bytes.restype = C.c_int32
+    lib.orc_compact_bytes.argtypes = [C.c_int32]
+    lib.orc_precision_words.restype = C.c_int32
+    lib.orc_precision_words.argtypes = [C.c_int32]
+    lib.orc_eval_expr.restype = C.c_int32
+    lib.orc_eval_expr.argtypes = [P, C.c_int32, C.c_int32, P, P, C.c_int64, C.c_int64, P, C.c_int32, P, P]
+    lib.orc_eval_expr_mt.restype = C.c_int32
+    lib.orc_eval_expr_mt.argtypes = [P, C.c_int32, C.c_int32, P, P, C.c_int64, P, C.c_int32, P, C.c_int32]
+    lib.orc_group_agg.restype = C.c_int32
+    lib.orc_group_agg.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, P, C.c_int64, C.c_int32, P]
+    lib.orc_query.restype = C.c_int32
+    lib.orc_query.argtypes = [P, C.c_int32, P, P, P, C.c_int32, P, C.c_int64, C.c_int32, P, C.c_int32]
+    lib.orc_division_int64.restype = None
+    lib.orc_division_int64.argtypes = [P, C.c_int64, P]
+    _lib = lib
+    return lib
+
+
+def _ptrs(bufs):
+    arr = (C.c_void_p * max(1, len(bufs)))()
+    keep = []
+    for i, b in enumerate(bufs):
+        cb = (C.c_char * len(b)).from_buffer_copy(b) if not isinstance(b, C.Array) else b
+        keep.append(cb)
+        arr[i] = C.cast(cb, C.c_void_p)
+    return arr, keep
+
+
+def eval_expr(built, root: int, cols: list[bytes], rows: int, out_bytes: int, threads: int = 1,
+              row_errors: bool = False):
+    """Evaluate `built.nodes` at `root` over host columns; returns
+    (bytes, err_word[, per-row error bytes])."""
+    lib = load()
+    arr, keep = _ptrs(cols)
+    out = (C.c_uint8 * max(1, rows * out_bytes))()
+    err = C.c_uint32(0)
+    if threads > 1 and not row_errors:
+        rc = lib.orc_eval_expr_mt(built.nodes, built.n_nodes, root, built.col_types, arr, rows, out, out_bytes,
+                                  C.byref(err), threads)
+        rerr = None
+    else:
+        rerr = (C.c_uint8 * max(1, rows))()
+        rc = lib.orc_eval_expr(built.nodes, built.n_nodes, root, built.col_types, arr, 0, rows, out, out_bytes,
+                               C.byref(err), rerr)
+    if rc != 0:
+        raise RuntimeError("oracle rejected the expression")
+    res = bytes(out)[:rows * out_bytes]
+    if row_errors:
+        return res, err.value, bytes(rerr)[:rows]
+    return res, err.value
+
+
+def group_agg(vals: bytes, value_bytes: int, scale: int, kind: int, gids: bytes, rows: int, n_groups: int) -> bytes:
+    lib = load()
+    width = 8 if kind == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES
+    out = (C.c_uint8 * max(1, n_groups * width))()
+    v = (C.c_char * max(1, len(vals))).from_buffer_copy(vals or b"\0")
+    g = (C.c_char * max(1, len(gids))).from_buffer_copy(gids or b"\0")
+    lib.orc_group_agg(v, value_bytes, scale, kind, g, rows, n_groups, out)
+    return bytes(out)[:n_groups * width]
+
+
+def query(built, aggs: list[tuple[int, int]], cols: list[bytes], gids: bytes, rows: int, n_groups: int,
+          threads: int = 1) -> list[bytes]:
+    """aggs: (kind, root) pairs; returns one output buffer per aggregate."""
+    lib = load()
+    arr, keep = _ptrs(cols)
+    qa = (abi.UpQueryAgg * len(aggs))()
+    outs = []
+    optr = (C.c_void_p * len(aggs))()
+    for i, (k, r) in enumerate(aggs):
+        qa[i].kind = k
+        qa[i].root = r
+        width = 8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES
+        o = (C.c_uint8 * max(1, n_groups * width))()
+        outs.append((o, width))
+        optr[i] = C.cast(o, C.c_void_p)
+    g = (C.c_char * max(1, len(gids))).from_buffer_copy(gids or b"\0")
+    lib.orc_query(built.nodes, built.n_nodes, built.col_types, arr, qa, len(aggs), g, rows, n_groups, optr,
+                  threads)
+    return [bytes(o)[:n_groups * w] for o, w in outs]
+
+
+def division_int64(sum_img: bytes, count: int) -> bytes:
+    lib = load()
+    out = (C.c_uint8 * abi.UP_AGG_DECIMAL_BYTES)()
+    s = (C.c_char * len(sum_img)).from_buffer_copy(sum_img)
+    lib.orc_division_int64(s, count, out)
+    return bytes(out)

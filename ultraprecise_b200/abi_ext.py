@@ -1,0 +1,16 @@
+"""Prototypes of the entry points declared in include/ultraprecise_util.h
+and include/ultraprecise_batch.h / ultraprecise_serve.h."""
+import ctypes as C
+
+_P = C.c_void_p
+_I32 = C.c_int32
+_I64 = C.c_int64
+_U64 = C.c_uint64
+
+SIGNATURES = {
+    "up_util_gen_digits": (_I32, [_P, _I64, _I32, _U64, _I32, _I32, _P]),
+    "up_util_gen_range": (_I32, [_P, _I64, _I32, _I64, _I64, _I64, _U64, _P]),
+    "up_util_flush_l2": (_I32, [_P, _I64, _P]),
+    "up_util_imad_peak": (_I32, [C.POINTER(C.c_double), _P]),
+    "up_util_compile_only": (_I32, [_P, _I32, _I32, _P, _I32, _I32, _P, _I32]),
+}

@@ -1,0 +1,416 @@
+// up_abi.cpp — the C entry points of libultraprecise.so (include/ultraprecise.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ultraprecise_util.h"
+#include "up_internal.h"
+#include "up_kernels.h"
+
+using namespace upi;
+
+namespace {
+
+// Host mirror of the device-side argument blocks emitted by the code
+// generator (KCol in up_dev.cuh; UpArgs / UpQArgs in up_codegen.cpp).
+struct HKCol {
+    const void* data;
+    const void* const* blocks;
+    const int64_t* prefix;
+    const int32_t* indices;
+    int32_t n_blocks;
+    int32_t value_bytes;
+};
+static_assert(sizeof(HKCol) == 40, "KCol layout");
+constexpr int kMaxCols = 16;
+constexpr int kMaxAggs = 16;
+struct HUpArgs {
+    HKCol col[kMaxCols];
+    int64_t rows;
+    uint8_t* out;
+    uint32_t* err;
+    int32_t vec_ok;
+    int32_t out_nullable;
+};
+static_assert(sizeof(HUpArgs) == 672, "UpArgs layout");
+struct HUpQArgs {
+    HKCol col[kMaxCols];
+    uint8_t* out[kMaxAggs];
+    int64_t rows;
+    const int32_t* gid;
+    uint32_t* acc;
+    uint64_t* cnt;
+    uint32_t* err;
+    int32_t n_groups;
+    int32_t vec_ok;
+};
+static_assert(sizeof(HUpQArgs) == 816, "UpQArgs layout");
+
+up_status cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();
+    up_status s = (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? UP_ERR_NO_DEVICE
+                  : (e == cudaErrorMemoryAllocation)                           ? UP_ERR_NO_MEMORY
+                                                                               : UP_ERR_CUDA;
+    return fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define UP_CUDA(call)                                  \
+    do {                                               \
+        cudaError_t e_ = (call);                       \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+struct ModCols {
+    std::vector<up_col_type> cols;
+};
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+up_status check_columns(const up_module* m, const up_column* in, int n_in, HKCol* kc, bool& all_contig,
+                        bool& vec_ok) {
+    const GeneratedModule& g = m->jm.gen;
+    if ((int)g.in_bytes.size() > n_in) return fail(UP_ERR_INVALID_ARG, "fewer input columns than compiled");
+    if (n_in > kMaxCols) return fail(UP_ERR_INVALID_ARG, "at most 16 input columns");
+    all_contig = true;
+    vec_ok = true;
+    for (int c = 0; c < (int)g.in_bytes.size(); c++) {
+        const up_column& col = in[c];
+        if (col.value_bytes != g.in_bytes[c])
+            return fail(UP_ERR_INVALID_ARG, "column " + std::to_string(c) + ": value_bytes " +
+                                                std::to_string(col.value_bytes) + " != compiled " +
+                                                std::to_string(g.in_bytes[c]));
+        if (!col.data && col.n_blocks <= 0) return fail(UP_ERR_INVALID_ARG, "column has neither data nor blocks");
+        if (col.n_blocks > 0 && (!col.blocks || !col.block_prefix))
+            return fail(UP_ERR_INVALID_ARG, "block column without block arrays");
+        kc[c].data = col.data;
+        kc[c].blocks = col.blocks;
+        kc[c].prefix = col.block_prefix;
+        kc[c].indices = col.indices;
+        kc[c].n_blocks = col.n_blocks > 0 ? col.n_blocks : 0;
+        kc[c].value_bytes = col.value_bytes;
+        if (col.n_blocks > 0 || col.indices || col.nullable || !col.data) all_contig = false;
+        if (!aligned16(col.data)) vec_ok = false;
+    }
+    return UP_OK;
+}
+
+int occupancy(void* kernel, int threads, int smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void*)kernel, threads, (size_t)smem) != cudaSuccess) {
+        cudaGetLastError();
+        n = 1;
+    }
+    return n < 1 ? 1 : n;
+}
+
+up_status set_smem(void* kernel, int smem) {
+    if (smem > 48 * 1024) {
+        UP_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    }
+    return UP_OK;
+}
+
+}  // namespace
+
+namespace upi {
+int sm_count_current() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+}  // namespace upi
+
+extern "C" {
+
+const char* up_status_string(up_status s) {
+    switch (s) {
+        case UP_OK: return "ok";
+        case UP_ERR_INVALID_ARG: return "invalid argument";
+        case UP_ERR_UNSUPPORTED: return "unsupported";
+        case UP_ERR_CUDA: return "CUDA error";
+        case UP_ERR_COMPILE: return "compile error";
+        case UP_ERR_NO_MEMORY: return "out of memory";
+        case UP_ERR_TIMEOUT: return "timeout";
+        case UP_ERR_QUEUE_FULL: return "queue full";
+        case UP_ERR_NOT_READY: return "not ready";
+        case UP_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* up_last_error_message(void) { return last_error(); }
+int32_t up_abi_version(void) { return UP_ABI_VERSION; }
+int32_t up_compact_bytes(int32_t p) { return compact_bytes(p); }
+int32_t up_precision_words(int32_t p) { return precision_words(p); }
+int32_t up_max_precision(void) { return kMaxPrecision; }
+
+up_status up_module_compile(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
+                            int32_t n_cols, const up_compile_opts* opts, up_module** out) {
+    if (!out) return fail(UP_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    GeneratedModule gen;
+    up_status st = generate_expr_module(nodes, n_nodes, root, cols, n_cols, opts, gen);
+    if (st != UP_OK) return st;
+    std::shared_ptr<JitKernelSet> ks;
+    st = jit_get(gen, ks);
+    if (st != UP_OK) return st;
+    up_module* m = new up_module();
+    m->jm.ks = ks;
+    m->jm.gen = std::move(gen);
+    m->is_query = false;
+    *out = m;
+    return UP_OK;
+}
+
+up_status up_module_result_type(const up_module* m, int32_t* precision, int32_t* scale, int32_t* value_bytes) {
+    if (!m) return fail(UP_ERR_INVALID_ARG, "module is NULL");
+    if (precision) *precision = m->jm.gen.out_precision;
+    if (scale) *scale = m->jm.gen.out_scale;
+    if (value_bytes) *value_bytes = m->jm.gen.out_bytes;
+    return UP_OK;
+}
+
+int64_t up_module_source(const up_module* m, char* buf, int64_t cap) {
+    if (!m) return -1;
+    const std::string& s = m->jm.gen.source;
+    if (buf && cap > 0) {
+        int64_t n = std::min<int64_t>(cap - 1, (int64_t)s.size());
+        memcpy(buf, s.data(), (size_t)n);
+        buf[n] = 0;
+    }
+    return (int64_t)s.size();
+}
+
+void up_module_release(up_module* m) { delete m; }
+
+int32_t up_module_cache_size(int32_t clear) { return jit_cache_size(clear != 0); }
+
+up_status up_expr_launch(up_module* m, const up_column* in, int32_t n_in, int64_t rows, void* out,
+                         uint32_t* err_word, void* stream) {
+    if (!m || m->is_query) return fail(UP_ERR_INVALID_ARG, "not an expression module");
+    if (rows < 0) return fail(UP_ERR_INVALID_ARG, "negative row count");
+    if (rows == 0) return UP_OK;
+    if (!out) return fail(UP_ERR_INVALID_ARG, "out is NULL");
+    if (n_in > 0 && !in) return fail(UP_ERR_INVALID_ARG, "inputs are NULL");
+    const GeneratedModule& g = m->jm.gen;
+    HUpArgs a;
+    memset(&a, 0, sizeof a);
+    bool contig = true, vec_ok = true;
+    up_status st = check_columns(m, in, n_in, a.col, contig, vec_ok);
+    if (st != UP_OK) return st;
+    a.rows = rows;
+    a.out = (uint8_t*)out;
+    a.err = err_word;
+    a.out_nullable = g.out_bytes != (g.out_is_compare ? 1 : compact_bytes(g.out_precision));
+    vec_ok = vec_ok && aligned16(out);
+    a.vec_ok = vec_ok ? 1 : 0;
+    const int sms = sm_count_current();
+    if (sms <= 0) return fail(UP_ERR_NO_DEVICE, "no CUDA device");
+    void* args[1] = {&a};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (contig && !a.out_nullable) {
+        void* k = jit_kernel(*m->jm.ks, "up_expr_tile");
+        st = set_smem(k, g.smem_bytes);
+        if (st != UP_OK) return st;
+        const int64_t ntiles = (rows + g.tile_rows - 1) / g.tile_rows;
+        const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, g.smem_bytes);
+        const unsigned grid = (unsigned)std::min<int64_t>(ntiles, cap);
+        UP_CUDA(cudaLaunchKernel((const void*)k, dim3(grid), dim3(g.block_threads), args, (size_t)g.smem_bytes, s));
+    } else {
+        void* k = jit_kernel(*m->jm.ks, "up_expr_generic");
+        const int64_t blocks = (rows + g.block_threads - 1) / g.block_threads;
+        const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, 0) * 4;
+        const unsigned grid = (unsigned)std::min<int64_t>(blocks, cap);
+        UP_CUDA(cudaLaunchKernel((const void*)k, dim3(grid), dim3(g.block_threads), args, 0, s));
+    }
+    return UP_OK;
+}
+
+up_status up_query_compile(const up_expr_node* nodes, int32_t n_nodes, const up_col_type* cols, int32_t n_cols,
+                           const up_query_agg* aggs, int32_t n_aggs, const up_compile_opts* opts, up_module** out) {
+    if (!out) return fail(UP_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    GeneratedModule gen;
+    up_status st = generate_query_module(nodes, n_nodes, cols, n_cols, aggs, n_aggs, opts, gen);
+    if (st != UP_OK) return st;
+    std::shared_ptr<JitKernelSet> ks;
+    st = jit_get(gen, ks);
+    if (st != UP_OK) return st;
+    up_module* m = new up_module();
+    m->jm.ks = ks;
+    m->jm.gen = std::move(gen);
+    m->is_query = true;
+    *out = m;
+    return UP_OK;
+}
+
+up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
+                          int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream) {
+    if (!m || !m->is_query) return fail(UP_ERR_INVALID_ARG, "not a query module");
+    if (rows < 0 || n_groups < 0) return fail(UP_ERR_INVALID_ARG, "negative size");
+    if (n_groups == 0) return UP_OK;
+    if (rows > 0 && !group_ids) return fail(UP_ERR_INVALID_ARG, "group ids are NULL");
+    if (!outs) return fail(UP_ERR_INVALID_ARG, "outputs are NULL");
+    const GeneratedModule& g = m->jm.gen;
+    HUpQArgs a;
+    memset(&a, 0, sizeof a);
+    bool contig = true, vec_ok = true;
+    up_status st = check_columns(m, in, n_in, a.col, contig, vec_ok);
+    if (st != UP_OK) return st;
+    for (int k = 0; k < g.n_aggs; k++) {
+        if (!outs[k]) return fail(UP_ERR_INVALID_ARG, "output " + std::to_string(k) + " is NULL");
+        a.out[k] = (uint8_t*)outs[k];
+    }
+    const int sms = sm_count_current();
+    if (sms <= 0) return fail(UP_ERR_NO_DEVICE, "no CUDA device");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t accw = (size_t)std::max(g.acc_words_per_group, 1);
+    // the int64 counts follow the accumulators: keep them 16-byte aligned
+    const size_t acc_bytes = (((size_t)n_groups * accw * 4u) + 15u) & ~(size_t)15u;
+    const size_t cnt_bytes = (size_t)n_groups * 8u;
+    void* scratch = nullptr;
+    UP_CUDA(cudaMallocAsync(&scratch, acc_bytes + cnt_bytes, s));
+    cudaError_t e = cudaMemsetAsync(scratch, 0, acc_bytes + cnt_bytes, s);
+    a.rows = rows;
+    a.gid = group_ids;
+    a.acc = (uint32_t*)scratch;
+    a.cnt = (uint64_t*)((uint8_t*)scratch + acc_bytes);
+    a.err = err_word;
+    a.n_groups = n_groups;
+    a.vec_ok = vec_ok ? 1 : 0;
+    void* args[1] = {&a};
+    if (e == cudaSuccess && rows > 0) {
+        void* k = jit_kernel(*m->jm.ks, "up_query_acc");
+        const int64_t blocks = (rows + g.block_threads - 1) / g.block_threads;
+        const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, 0) * 4;
+        e = cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(blocks, cap)), dim3(g.block_threads),
+                             args, 0, s);
+    }
+    if (e == cudaSuccess) {
+        void* k = jit_kernel(*m->jm.ks, "up_query_fin");
+        e = cudaLaunchKernel((const void*)k, dim3((unsigned)((n_groups + 255) / 256)), dim3(256), args, 0, s);
+    }
+    cudaError_t e2 = cudaFreeAsync(scratch, s);
+    if (e != cudaSuccess) return cuda_fail(e, "query launch");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaFreeAsync");
+    return UP_OK;
+}
+
+up_status up_group_agg(const up_column* vals, const int32_t* kinds, int32_t n_vals, const int32_t* group_ids,
+                       int32_t n_groups, int64_t rows, void* const* outs, uint32_t* err_word, void* stream) {
+    if (n_vals <= 0 || n_vals > kMaxAggs) return fail(UP_ERR_INVALID_ARG, "1..16 aggregates");
+    if (!vals || !kinds) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    std::vector<up_expr_node> nodes(n_vals);
+    std::vector<up_col_type> cols(n_vals);
+    std::vector<up_query_agg> aggs(n_vals);
+    for (int k = 0; k < n_vals; k++) {
+        memset(&nodes[k], 0, sizeof(up_expr_node));
+        nodes[k].kind = UP_NODE_COLUMN;
+        nodes[k].left = nodes[k].right = -1;
+        nodes[k].column = k;
+        nodes[k].precision = vals[k].precision;
+        nodes[k].scale = vals[k].scale;
+        cols[k].precision = vals[k].precision;
+        cols[k].scale = vals[k].scale;
+        cols[k].nullable = vals[k].nullable;
+        aggs[k].kind = kinds[k];
+        aggs[k].root = k;
+    }
+    up_module* m = nullptr;
+    up_status st = up_query_compile(nodes.data(), n_vals, cols.data(), n_vals, aggs.data(), n_vals, nullptr, &m);
+    if (st != UP_OK) return st;
+    st = up_query_launch(m, vals, n_vals, rows, group_ids, n_groups, outs, err_word, stream);
+    up_module_release(m);
+    return st;
+}
+
+up_status up_aggregate_column_data(const up_column* src, int32_t kind, const int32_t* associated,
+                                   const int32_t* group_starts, int32_t n_groups, int64_t rows, void* out,
+                                   uint32_t* err_word, void* stream) {
+    if (!src || !out) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    if (n_groups < 0 || rows < 0) return fail(UP_ERR_INVALID_ARG, "negative size");
+    if (n_groups == 0) return UP_OK;
+    if (rows > 0 && !group_starts) return fail(UP_ERR_INVALID_ARG, "group starts are NULL");
+    if (associated && src->indices) return fail(UP_ERR_UNSUPPORTED, "column already has an indirection");
+    cudaStream_t s = (cudaStream_t)stream;
+    int32_t* gid = nullptr;
+    if (rows > 0) {
+        UP_CUDA(cudaMallocAsync((void**)&gid, (size_t)rows * 4u, s));
+        cudaError_t e = launch_fill_segment_gids(group_starts, n_groups, rows, gid, s);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(gid, s);
+            return cuda_fail(e, "fill segment ids");
+        }
+    }
+    up_column c = *src;
+    if (associated) c.indices = associated;
+    void* outs[1] = {out};
+    up_status st = up_group_agg(&c, &kind, 1, gid, n_groups, rows, outs, err_word, stream);
+    if (gid) cudaFreeAsync(gid, s);
+    return st;
+}
+
+up_status up_division_int64(const void* sums, const int64_t* counts, int32_t n, void* out, void* stream) {
+    if (n < 0) return fail(UP_ERR_INVALID_ARG, "negative size");
+    if (n == 0) return UP_OK;
+    if (!sums || !counts || !out) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    UP_CUDA(launch_division_int64((const uint8_t*)sums, counts, n, (uint8_t*)out, (cudaStream_t)stream));
+    return UP_OK;
+}
+
+up_status up_group_ids_from_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys, int64_t rows,
+                                 int32_t* group_ids, int32_t* n_groups, void* group_keys, void* stream) {
+    if (!key_cols || !key_bytes || !group_ids || !n_groups) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    if (n_keys < 1 || n_keys > 4) return fail(UP_ERR_INVALID_ARG, "1..4 key columns");
+    int total = 0;
+    for (int k = 0; k < n_keys; k++) {
+        if (key_bytes[k] < 1) return fail(UP_ERR_INVALID_ARG, "key width < 1");
+        total += key_bytes[k];
+    }
+    if (total > 2) return fail(UP_ERR_UNSUPPORTED, "direct key table supports at most 2 key bytes in total");
+    cudaStream_t s = (cudaStream_t)stream;
+    UP_CUDA(launch_group_ids_small_keys(key_cols, key_bytes, n_keys, rows, group_ids, n_groups, group_keys, s));
+    return UP_OK;
+}
+
+up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
+                               int32_t n_cols, int32_t query, const up_query_agg* aggs, int32_t n_aggs) {
+    GeneratedModule gen;
+    up_status st = query ? generate_query_module(nodes, n_nodes, cols, n_cols, aggs, n_aggs, nullptr, gen)
+                         : generate_expr_module(nodes, n_nodes, root, cols, n_cols, nullptr, gen);
+    if (st != UP_OK) return st;
+    std::vector<char> cubin;
+    return jit_compile_cubin(gen.source, cubin);
+}
+
+up_status up_device_query(int32_t device, up_device_info* info) {
+    if (!info) return fail(UP_ERR_INVALID_ARG, "info is NULL");
+    memset(info, 0, sizeof *info);
+    cudaDeviceProp p;
+    UP_CUDA(cudaGetDeviceProperties(&p, device));
+    info->sm_count = p.multiProcessorCount;
+    info->cc_major = p.major;
+    info->cc_minor = p.minor;
+    strncpy(info->name, p.name, sizeof(info->name) - 1);
+    int cur = 0;
+    UP_CUDA(cudaGetDevice(&cur));
+    if (cur == device) {
+        size_t fr = 0, tot = 0;
+        UP_CUDA(cudaMemGetInfo(&fr, &tot));
+        info->free_bytes = (int64_t)fr;
+        info->total_bytes = (int64_t)tot;
+    }
+    return UP_OK;
+}
+
+}  // extern "C"

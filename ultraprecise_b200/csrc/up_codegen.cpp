@@ -1,0 +1,475 @@
+// up_codegen.cpp — typed expression DAG -> CUDA C++ source for NVRTC.
+//
+// Plays the role of the reference's expression codegen
+// (AriesCommonExpr::StringForDynamicCode, AriesCommonExpr.cpp:163-304, and
+// AEExprCalcNode::GenerateCudaFunction / GenerateLoadDataCode /
+// GenSaveDataCode, AriesExprCalcNode.cpp:76-106, 1285-1428), but emits
+// straight-line limb code with every node's limb count and scale fixed at
+// compile time instead of instantiating one AriesDecimal<LEN> for all nodes.
+#include <algorithm>
+#include <cstdio>
+#include <map>
+#include <set>
+#include <sstream>
+
+#include "up_internal.h"
+
+namespace upi {
+
+namespace {
+
+std::string hex32(uint32_t v) {
+    char b[16];
+    snprintf(b, sizeof b, "0x%08xu", v);
+    return b;
+}
+
+std::string limbs_init(const Big& x, int n) {
+    std::string s = "{";
+    for (int i = 0; i < n; i++) {
+        if (i) s += ", ";
+        s += hex32(i < (int)x.m.size() ? x.m[i] : 0u);
+    }
+    return s + "}";
+}
+
+bool is_compare_kind(int k) { return k >= UP_NODE_LT && k <= UP_NODE_NE; }
+
+// Emits the body of a per-row evaluation function for a set of nodes.
+struct Emitter {
+    const up_expr_node* nodes;
+    const up_col_type* cols;
+    const std::vector<NodeFacts>& f;
+    std::ostringstream body;
+    std::set<int> p10;
+    int tmp = 0;
+
+    Emitter(const up_expr_node* n, const up_col_type* c, const std::vector<NodeFacts>& facts)
+        : nodes(n), cols(c), f(facts) {}
+
+    std::string p10_name(int k) {
+        p10.insert(k);
+        return "P10_" + std::to_string(k);
+    }
+
+    std::string v(int k) { return "v" + std::to_string(k); }
+    std::string s(int k) { return "s" + std::to_string(k); }
+
+    // name of an array holding node a's magnitude at scale sc (sc >= scale(a))
+    std::string aligned(int a, int sc) {
+        const NodeFacts& fa = f[a];
+        if (sc == fa.scale) return v(a);
+        const int d = sc - fa.scale;
+        Big p = big_pow10(d);
+        const int L = limbs_for_bits(fa.bits + big_bitlen(p));
+        std::string t = "t" + std::to_string(tmp++);
+        body << "    u32 " << t << "[" << L << "];\n";
+        if (p.m.size() == 1) body << "    mul_u32(" << t << ", " << v(a) << ", " << hex32(p.m[0]) << ");\n";
+        else body << "    mul(" << t << ", " << v(a) << ", " << p10_name(d) << ");\n";
+        return t;
+    }
+
+    void node(int k) {
+        const up_expr_node& nd = nodes[k];
+        const NodeFacts& fk = f[k];
+        const int L = fk.limbs;
+        body << "    // node " << k << ": kind " << nd.kind << ", scale " << fk.scale << ", <= " << fk.bits
+             << " bits\n";
+        switch (nd.kind) {
+            case UP_NODE_COLUMN: {
+                const int B = compact_bytes(cols[nd.column].precision);
+                body << "    u32 " << v(k) << "[" << L << "]; u32 " << s(k) << ";\n";
+                body << "    if (TILE) ld_compact_words<" << B << ", " << L << ">(in" << nd.column << ", " << v(k)
+                     << ", " << s(k) << ");\n";
+                body << "    else ld_compact_bytes<" << B << ", " << L << ">(in" << nd.column << ", " << v(k)
+                     << ", " << s(k) << ");\n";
+                break;
+            }
+            case UP_NODE_CONST: {
+                Big c;
+                c.m.assign(nd.const_limbs, nd.const_limbs + nd.const_nlimbs);
+                big_trim(c);
+                body << "    const u32 " << v(k) << "[" << L << "] = " << limbs_init(c, L) << "; u32 " << s(k)
+                     << " = " << (nd.const_sign ? 1 : 0) << "u;\n";
+                break;
+            }
+            case UP_NODE_INT: {
+                uint64_t mag = nd.int_value < 0 ? (uint64_t)(-(nd.int_value + 1)) + 1u : (uint64_t)nd.int_value;
+                body << "    const u32 " << v(k) << "[" << L << "] = " << limbs_init(big_from_u64(mag), L)
+                     << "; u32 " << s(k) << " = " << (nd.int_value < 0 ? 1 : 0) << "u;\n";
+                break;
+            }
+            case UP_NODE_ADD:
+            case UP_NODE_SUB: {
+                std::string A = aligned(nd.left, fk.scale);
+                std::string Bn = aligned(nd.right, fk.scale);
+                body << "    u32 " << v(k) << "[" << L << "]; u32 " << s(k) << ";\n";
+                body << "    add_signed(" << v(k) << ", " << s(k) << ", " << A << ", " << s(nd.left) << ", " << Bn
+                     << ", " << s(nd.right) << (nd.kind == UP_NODE_SUB ? " ^ 1u" : "") << ");\n";
+                break;
+            }
+            case UP_NODE_MUL:
+                body << "    u32 " << v(k) << "[" << L << "]; mul(" << v(k) << ", " << v(nd.left) << ", "
+                     << v(nd.right) << "); u32 " << s(k) << " = " << s(nd.left) << " ^ " << s(nd.right) << ";\n";
+                break;
+            case UP_NODE_DIV: {
+                const int sh = f[nd.right].scale + 4;
+                Big p = big_pow10(sh);
+                const int np = (int)p.m.size();
+                char w[40];
+                snprintf(w, sizeof w, "0x%016llxull", (unsigned long long)big_low64(p));
+                body << "    u32 " << v(k) << "[" << L << "]; u32 " << s(k) << ";\n";
+                body << "    err |= div_round<" << L << ", " << f[nd.left].limbs << ", " << f[nd.right].limbs << ", "
+                     << np << ", " << sh << "u, " << w << ">(" << v(k) << ", " << s(k) << ", " << v(nd.left)
+                     << ", " << s(nd.left) << ", " << v(nd.right) << ", " << s(nd.right) << ", " << p10_name(sh)
+                     << ");\n";
+                break;
+            }
+            case UP_NODE_MOD:
+                body << "    u32 " << v(k) << "[" << L << "]; u32 " << s(k) << ";\n";
+                body << "    err |= mod(" << v(k) << ", " << s(k) << ", " << v(nd.left) << ", " << s(nd.left) << ", "
+                     << v(nd.right) << ", " << s(nd.right) << ");\n";
+                break;
+            case UP_NODE_RESCALE: {
+                const int sa = f[nd.left].scale;
+                body << "    u32 " << v(k) << "[" << L << "]; u32 " << s(k) << " = " << s(nd.left) << ";\n";
+                if (nd.scale >= sa) {
+                    std::string A = aligned(nd.left, nd.scale);
+                    body << "    copy_ext(" << v(k) << ", " << A << ");\n";
+                } else {
+                    body << "    trunc_div_pow10(" << v(k) << ", " << v(nd.left) << ", " << p10_name(sa - nd.scale)
+                         << ");\n";
+                }
+                break;
+            }
+            default: {
+                // comparison
+                const int sc = std::max(f[nd.left].scale, f[nd.right].scale);
+                std::string A = aligned(nd.left, sc);
+                std::string Bn = aligned(nd.right, sc);
+                body << "    const u32 c" << k << " = compare(" << (nd.kind - UP_NODE_LT) << ", " << A << ", "
+                     << s(nd.left) << ", " << Bn << ", " << s(nd.right) << ");\n";
+                return;
+            }
+        }
+        if (nd.reverse) body << "    " << s(k) << " ^= 1u;\n";
+    }
+
+    std::string constants() {
+        std::ostringstream o;
+        for (int k : p10) {
+            Big p = big_pow10(k);
+            o << "    const u32 P10_" << k << "[" << p.m.size() << "] = " << limbs_init(p, (int)p.m.size()) << ";\n";
+        }
+        return o.str();
+    }
+};
+
+std::string kargs_source() {
+    return R"(
+#define UP_MAX_COLS 16
+#define UP_MAX_AGGS 16
+struct UpArgs {
+    KCol col[UP_MAX_COLS];
+    i64 rows;
+    u8* out;
+    u32* err;
+    int vec_ok;
+    int out_nullable;
+};
+struct UpQArgs {
+    KCol col[UP_MAX_COLS];
+    u8* out[UP_MAX_AGGS];
+    i64 rows;
+    const int* gid;
+    u32* acc;
+    u64* cnt;
+    u32* err;
+    int n_groups;
+    int vec_ok;
+};
+)";
+}
+
+std::string params_decl(const std::vector<int>& used_cols) {
+    std::string p;
+    for (int c : used_cols) p += "const u8* __restrict__ in" + std::to_string(c) + ", ";
+    return p;
+}
+
+}  // namespace
+
+// --------------------------------------------------- expression modules
+up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
+                               int n_cols, const up_compile_opts* opts, GeneratedModule& out) {
+    if (!nodes || n_nodes <= 0) return fail(UP_ERR_INVALID_ARG, "empty expression");
+    if (n_cols < 0 || n_cols > 16) return fail(UP_ERR_INVALID_ARG, "at most 16 input columns");
+    if (n_cols > 0 && !cols) return fail(UP_ERR_INVALID_ARG, "column types missing");
+    std::vector<NodeFacts> f;
+    std::vector<int> topo;
+    up_status st = analyze_nodes(nodes, n_nodes, cols, n_cols, f, topo, {root});
+    if (st != UP_OK) return st;
+    const up_expr_node& rn = nodes[root];
+    const bool cmp_root = is_compare_kind(rn.kind);
+    int out_p = cmp_root ? 1 : rn.precision;
+    int out_s = cmp_root ? 0 : f[root].scale;
+    int BO = cmp_root ? 1 : compact_bytes(out_p);
+    if (!cmp_root && BO < 1) return fail(UP_ERR_INVALID_ARG, "root precision not set (run up_expr_derive_types)");
+    for (int k : topo) {
+        if (f[k].limbs > 512) return fail(UP_ERR_UNSUPPORTED, "intermediate wider than 16384 bits");
+    }
+
+    std::vector<int> used;
+    bool any_nullable = false;
+    for (int k : topo)
+        if (nodes[k].kind == UP_NODE_COLUMN) {
+            if (std::find(used.begin(), used.end(), nodes[k].column) == used.end()) used.push_back(nodes[k].column);
+            any_nullable |= cols[nodes[k].column].nullable != 0;
+        }
+    std::sort(used.begin(), used.end());
+
+    Emitter em(nodes, cols, f);
+    for (int k : topo) em.node(k);
+
+    const int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
+    int R = T;
+    int row_bytes = BO;
+    for (int c : used) row_bytes += compact_bytes(cols[c].precision);
+    // keep a tile within ~48 KB so several CTAs share an SM
+    while (R > 32 && (long)R * row_bytes > 48 * 1024) R /= 2;
+
+    std::ostringstream src;
+    src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << kargs_source();
+    src << "template <bool TILE>\nUP_DI u32 up_row(" << params_decl(used) << "u8* __restrict__ out) {\n";
+    src << "    u32 err = 0u;\n" << em.constants() << em.body.str();
+    if (cmp_root) {
+        src << "    out[0] = (u8)c" << root << ";\n";
+    } else if (BO % 4 == 0) {
+        src << "    if (TILE) err |= st_compact_words<" << BO << ">(out, v" << root << ", s" << root << ");\n";
+        src << "    else err |= st_compact_bytes<" << BO << ">(out, v" << root << ", s" << root << ");\n";
+    } else {
+        src << "    err |= st_compact_bytes<" << BO << ">(out, v" << root << ", s" << root << ");\n";
+    }
+    src << "    return err;\n}\n\n";
+
+    // tile kernel: contiguous columns, staged through shared memory
+    std::vector<int> off;
+    int smem = 0;
+    for (int c : used) {
+        off.push_back(smem);
+        smem += ((R * compact_bytes(cols[c].precision) + 16 + 15) / 16) * 16;
+    }
+    const int off_out = smem;
+    smem += ((R * BO + 16 + 15) / 16) * 16;
+
+    src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_tile(const UpArgs a) {\n";
+    src << "    extern __shared__ __align__(16) u8 sm[];\n";
+    src << "    constexpr int R = " << R << ";\n";
+    src << "    const i64 ntiles = (a.rows + R - 1) / R;\n    u32 err = 0u;\n";
+    src << "    for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x) {\n";
+    src << "        const i64 row0 = t * (i64)R;\n";
+    src << "        const int nr = (a.rows - row0) < R ? (int)(a.rows - row0) : R;\n";
+    for (size_t i = 0; i < used.size(); i++) {
+        int c = used[i];
+        int B = compact_bytes(cols[c].precision);
+        src << "        tile_copy_in(sm + " << off[i] << ", a.col[" << c << "].data + row0 * " << B << ", nr * " << B
+            << ", a.vec_ok != 0);\n";
+    }
+    src << "        __syncthreads();\n";
+    src << "        for (int r = threadIdx.x; r < nr; r += blockDim.x)\n";
+    src << "            err |= up_row<true>(";
+    for (size_t i = 0; i < used.size(); i++) {
+        int B = compact_bytes(cols[used[i]].precision);
+        src << "sm + " << off[i] << " + r * " << B << ", ";
+    }
+    src << "sm + " << off_out << " + r * " << BO << ");\n";
+    src << "        __syncthreads();\n";
+    src << "        tile_copy_out(a.out + row0 * " << BO << ", sm + " << off_out << ", nr * " << BO
+        << ", a.vec_ok != 0);\n";
+    src << "        __syncthreads();\n    }\n";
+    src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
+    src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
+
+    // generic kernel: blocks, indirection, nullable values
+    const int OB = BO + (any_nullable ? 1 : 0);
+    src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_generic(const UpArgs a) {\n";
+    src << "    u32 err = 0u;\n";
+    src << "    const i64 stride = (i64)gridDim.x * blockDim.x;\n";
+    src << "    for (i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x; row < a.rows; row += stride) {\n";
+    src << "        u8* o = a.out + row * " << OB << ";\n";
+    src << "        bool isnull = false;\n";
+    for (int c : used) {
+        src << "        const u8* in" << c << " = col_ptr(a.col[" << c << "], row);\n";
+        src << "        if (in" << c << " == nullptr) isnull = true;\n";
+        if (cols[c].nullable) {
+            src << "        else { if (in" << c << "[0] == 0) isnull = true; in" << c << " += 1; }\n";
+        }
+    }
+    if (any_nullable) {
+        src << "        o[0] = isnull ? 0 : 1;\n";
+        src << "        if (isnull) { for (int i = 0; i < " << BO << "; i++) o[1 + i] = 0; continue; }\n";
+        src << "        o += 1;\n";
+    } else {
+        src << "        if (isnull) { err |= ERR_DOMAIN; for (int i = 0; i < " << BO << "; i++) o[i] = 0; continue; }\n";
+    }
+    src << "        err |= up_row<false>(";
+    for (int c : used) src << "in" << c << ", ";
+    src << "o);\n    }\n";
+    src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
+    src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n";
+
+    out.source = src.str();
+    out.kernels = {"up_expr_tile", "up_expr_generic"};
+    out.out_precision = out_p;
+    out.out_scale = out_s;
+    out.out_bytes = OB;
+    out.out_is_compare = cmp_root;
+    out.block_threads = T;
+    out.tile_rows = R;
+    out.smem_bytes = smem;
+    out.in_bytes.assign(n_cols, 0);
+    for (int c = 0; c < n_cols; c++) out.in_bytes[c] = compact_bytes(cols[c].precision) + (cols[c].nullable ? 1 : 0);
+    return UP_OK;
+}
+
+// ------------------------------------------------------ query modules
+// Fused expression + grouped aggregation: every aggregate's expression is
+// evaluated per row and added exactly into per-group two's complement
+// accumulators (SUM/AVG), with a per-group row count; a second kernel turns
+// the accumulators into the reference's 133-byte nullable_type<Decimal>
+// images (AggregateColumnData SUM, AriesSqlOperator_group.cu:360-424, and
+// DivisionInt64 AVG, AriesSqlOperator_helpers.cu:717-763).
+up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up_col_type* cols, int n_cols,
+                                const up_query_agg* aggs, int n_aggs, const up_compile_opts* opts,
+                                GeneratedModule& out) {
+    if (!nodes || n_nodes <= 0) return fail(UP_ERR_INVALID_ARG, "empty query");
+    if (n_aggs <= 0 || n_aggs > 16) return fail(UP_ERR_INVALID_ARG, "1..16 aggregates");
+    if (n_cols < 0 || n_cols > 16) return fail(UP_ERR_INVALID_ARG, "at most 16 input columns");
+    std::vector<int> roots;
+    for (int a = 0; a < n_aggs; a++) {
+        int k = aggs[a].kind;
+        if (k != UP_AGG_COUNT && k != UP_AGG_SUM && k != UP_AGG_AVG)
+            return fail(UP_ERR_INVALID_ARG, "unknown aggregate kind");
+        if (k != UP_AGG_COUNT) roots.push_back(aggs[a].root);
+    }
+    std::vector<NodeFacts> f;
+    std::vector<int> topo;
+    if (!roots.empty()) {
+        up_status st = analyze_nodes(nodes, n_nodes, cols, n_cols, f, topo, roots);
+        if (st != UP_OK) return st;
+    }
+    for (int r : roots)
+        if (f[r].is_compare) return fail(UP_ERR_INVALID_ARG, "cannot sum a comparison");
+
+    std::vector<int> used;
+    for (int k : topo)
+        if (nodes[k].kind == UP_NODE_COLUMN &&
+            std::find(used.begin(), used.end(), nodes[k].column) == used.end())
+            used.push_back(nodes[k].column);
+    std::sort(used.begin(), used.end());
+
+    out.n_aggs = n_aggs;
+    out.agg_kind.clear();
+    out.agg_scale.clear();
+    out.agg_acc_limbs.clear();
+    out.agg_acc_offset.clear();
+    int accw = 0;
+    for (int a = 0; a < n_aggs; a++) {
+        out.agg_kind.push_back(aggs[a].kind);
+        if (aggs[a].kind == UP_AGG_COUNT) {
+            out.agg_scale.push_back(0);
+            out.agg_acc_limbs.push_back(0);
+            out.agg_acc_offset.push_back(0);
+            continue;
+        }
+        const NodeFacts& fr = f[aggs[a].root];
+        // one sign bit + up to 2^40 rows of headroom above the value bound
+        const int nacc = limbs_for_bits(fr.bits + 1 + 40);
+        out.agg_scale.push_back(fr.scale);
+        out.agg_acc_limbs.push_back(nacc);
+        out.agg_acc_offset.push_back(accw);
+        accw += nacc;
+    }
+    out.acc_words_per_group = accw;
+
+    Emitter em(nodes, cols, f);
+    for (int k : topo) em.node(k);
+
+    const int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
+    std::ostringstream src;
+    src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << kargs_source();
+    src << "template <bool TILE>\nUP_DI u32 up_qrow(" << params_decl(used) << "u32* __restrict__ acc) {\n";
+    src << "    u32 err = 0u;\n" << em.constants() << em.body.str();
+    for (int a = 0; a < n_aggs; a++) {
+        if (aggs[a].kind == UP_AGG_COUNT) continue;
+        int r = aggs[a].root;
+        src << "    atomic_acc_add<" << out.agg_acc_limbs[a] << ">(acc + " << out.agg_acc_offset[a] << ", v" << r
+            << ", s" << r << ");\n";
+    }
+    src << "    return err;\n}\n\n";
+
+    src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_query_acc(const UpQArgs a) {\n";
+    src << "    u32 err = 0u;\n";
+    src << "    const i64 stride = (i64)gridDim.x * blockDim.x;\n";
+    src << "    for (i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x; row < a.rows; row += stride) {\n";
+    src << "        const int g = a.gid[row];\n";
+    src << "        if ((unsigned)g >= (unsigned)a.n_groups) { err |= ERR_DOMAIN; continue; }\n";
+    src << "        atomicAdd(a.cnt + g, 1ull);\n";
+    src << "        bool isnull = false;\n";
+    for (int c : used) {
+        src << "        const u8* in" << c << " = col_ptr(a.col[" << c << "], row);\n";
+        src << "        if (in" << c << " == nullptr) isnull = true;\n";
+        if (cols[c].nullable)
+            src << "        else { if (in" << c << "[0] == 0) isnull = true; in" << c << " += 1; }\n";
+    }
+    src << "        if (isnull) continue;\n";
+    src << "        err |= up_qrow<false>(";
+    for (int c : used) src << "in" << c << ", ";
+    src << "a.acc + (i64)g * " << std::max(accw, 1) << ");\n    }\n";
+    src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
+    src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
+
+    src << "extern \"C\" __global__ void __launch_bounds__(256) up_query_fin(const UpQArgs a) {\n";
+    src << "    const int g = blockIdx.x * blockDim.x + threadIdx.x;\n";
+    src << "    if (g >= a.n_groups) return;\n";
+    src << "    const u64 cnt = a.cnt[g];\n";
+    src << "    const u32* acc = a.acc + (i64)g * " << std::max(accw, 1) << ";\n";
+    src << "    const u32 P10_4[1] = {10000u};\n";
+    for (int a = 0; a < n_aggs; a++) {
+        int k = aggs[a].kind;
+        src << "    {\n";
+        if (k == UP_AGG_COUNT) {
+            src << "        ((i64*)a.out[" << a << "])[g] = (i64)cnt;\n";
+        } else {
+            int n = out.agg_acc_limbs[a];
+            src << "        u32 m[" << n << "];\n";
+            src << "        for (int i = 0; i < " << n << "; i++) m[i] = acc[" << out.agg_acc_offset[a] << " + i];\n";
+            src << "        const u32 neg = m[" << n - 1 << "] >> 31;\n";
+            src << "        if (neg) negate(m);\n";
+            src << "        u8* img = a.out[" << a << "] + (i64)g * 133;\n";
+            if (k == UP_AGG_SUM) {
+                src << "        agg_image(img, cnt > 0 ? 1u : 0u, neg, " << out.agg_scale[a] << "u, m);\n";
+            } else {
+                int nq = n + 1;
+                src << "        if (cnt == 0) { agg_image(img, 0u, 0u, " << out.agg_scale[a] + 4 << "u, m); }\n";
+                src << "        else {\n";
+                src << "            const u32 c2[2] = {(u32)cnt, (u32)(cnt >> 32)};\n";
+                src << "            u32 q[" << nq << "]; u32 sq;\n";
+                src << "            div_round<" << nq << ", " << n << ", 2, 1, 4u, 10000ull>(q, sq, m, neg, c2, 0u, P10_4);\n";
+                src << "            agg_image(img, 1u, sq, " << out.agg_scale[a] + 4 << "u, q);\n";
+                src << "        }\n";
+            }
+        }
+        src << "    }\n";
+    }
+    src << "}\n";
+
+    out.source = src.str();
+    out.kernels = {"up_query_acc", "up_query_fin"};
+    out.block_threads = T;
+    out.in_bytes.assign(n_cols, 0);
+    for (int c = 0; c < n_cols; c++) out.in_bytes[c] = compact_bytes(cols[c].precision) + (cols[c].nullable ? 1 : 0);
+    return UP_OK;
+}
+
+}  // namespace upi

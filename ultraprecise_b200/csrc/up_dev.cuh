@@ -1,0 +1,598 @@
+// up_dev.cuh — device arithmetic on compact decimals for sm_100a.
+//
+// Compiled two ways: embedded into every NVRTC-generated expression kernel,
+// and included by the precompiled .cu files.  Uses no standard headers.
+//
+// Values are sign-magnitude: a little-endian base-2^32 magnitude held in a
+// fixed-size register array whose length is a compile-time bound derived from
+// the operands' bit widths, plus a sign word; the scale is static (it is part
+// of the expression type), so it never appears at run time.
+//
+// Semantics follow UltraPrecise's AriesDecimal<LEN> (src/datatypes/
+// AriesDecimal.hxx) with LEN large enough that nothing is truncated:
+//   add/sub sign rules    AriesDecimal.hxx:171-289
+//   multiply              AriesDecimal.hxx:316-404  (sign XOR: -x*0 = -0)
+//   divide                AriesDecimal.hxx:581-626, 748-878 (three branches)
+//   compare               AriesDecimal.hxx:458-570, 1023-1061
+//   compact load/store    AriesDecimal.hxx:105-114, 308-313; decimal.hxx:91-92
+#ifndef UP_DEV_CUH_
+#define UP_DEV_CUH_
+
+namespace up {
+
+typedef unsigned int u32;
+typedef unsigned long long u64;
+typedef long long i64;
+typedef unsigned char u8;
+
+#define UP_DI __device__ __forceinline__
+
+enum : u32 { ERR_OVERFLOW = 1u, ERR_DIV0 = 2u, ERR_DOMAIN = 4u };
+
+// ----------------------------------------------------------------- limbs
+template <int N>
+UP_DI u32 at(const u32 (&a)[N], int i) {
+    return (i >= 0 && i < N) ? a[(i >= 0 && i < N) ? i : 0] : 0u;
+}
+
+template <int N>
+UP_DI void zero(u32 (&r)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = 0u;
+}
+
+template <int N, int M>
+UP_DI void copy_ext(u32 (&r)[N], const u32 (&a)[M]) {
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = at(a, i);
+}
+
+template <int N>
+UP_DI bool is_zero(const u32 (&a)[N]) {
+    u32 o = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) o |= a[i];
+    return o == 0u;
+}
+
+// number of significant bits (0 for zero)
+template <int N>
+UP_DI u32 bitlen(const u32 (&a)[N]) {
+    u32 r = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) r = a[i] ? 32u * i + 32u - (u32)__clz(a[i]) : r;
+    return r;
+}
+
+// -1, 0, 1 comparing magnitudes
+template <int NA, int NB>
+UP_DI int cmp(const u32 (&a)[NA], const u32 (&b)[NB]) {
+    constexpr int M = NA > NB ? NA : NB;
+    int r = 0;
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+        u32 x = at(a, i), y = at(b, i);
+        r = x != y ? (x < y ? -1 : 1) : r;
+    }
+    return r;
+}
+
+// r = a + b over N limbs; returns the carry out of limb N-1
+template <int N, int NA, int NB>
+UP_DI u32 add(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
+    u64 c = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        c += (u64)at(a, i) + at(b, i);
+        r[i] = (u32)c;
+        c >>= 32;
+    }
+    return (u32)c;
+}
+
+// r = a - b over N limbs (two's complement); returns 1 when a < b
+template <int N, int NA, int NB>
+UP_DI u32 sub(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
+    u64 c = 1;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        c += (u64)at(a, i) + (u64)(~at(b, i));
+        r[i] = (u32)c;
+        c >>= 32;
+    }
+    return (u32)(c ^ 1u);
+}
+
+template <int N>
+UP_DI void negate(u32 (&r)[N]) {
+    u64 c = 1;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        c += (u64)(~r[i]);
+        r[i] = (u32)c;
+        c >>= 32;
+    }
+}
+
+// r += k (small), over N limbs
+template <int N>
+UP_DI void add_small(u32 (&r)[N], u32 k) {
+    u64 c = k;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        c += r[i];
+        r[i] = (u32)c;
+        c >>= 32;
+    }
+}
+
+// Signed add with AriesDecimal operator+= rules (AriesDecimal.hxx:171-223):
+// equal signs add magnitudes and keep the sign; different signs subtract the
+// smaller magnitude from the larger, the sign follows the larger, and equal
+// magnitudes give +0.  Subtraction is this with b's sign flipped (the
+// operator-= rules, AriesDecimal.hxx:234-289, reduce to exactly that).
+template <int N, int NA, int NB>
+UP_DI void add_signed(u32 (&r)[N], u32& sr, const u32 (&a)[NA], u32 sa, const u32 (&b)[NB], u32 sb) {
+    const bool same = sa == sb;
+    const u32 x = same ? 0u : 0xffffffffu;
+    u64 c = same ? 0u : 1u;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        c += (u64)at(a, i) + (u64)(at(b, i) ^ x);
+        r[i] = (u32)c;
+        c >>= 32;
+    }
+    const bool neg = !same && c == 0u;  // a < b
+    if (neg) negate(r);
+    const bool nz = !is_zero(r);
+    sr = same ? sa : (nz ? (neg ? sb : (sb ^ 1u)) : 0u);
+}
+
+// r = a * b (low N limbs of the product)
+template <int N, int NA, int NB>
+UP_DI void mul(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
+    zero(r);
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+        if (i >= N) break;
+        u64 c = 0;
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+            if (i + j < N) {
+                u64 t = (u64)a[i] * b[j] + r[i + j] + c;
+                r[i + j] = (u32)t;
+                c = t >> 32;
+            }
+        }
+        if (i + NB < N) r[i + NB] = (u32)c;
+    }
+}
+
+// r = a * k (k one limb)
+template <int N, int NA>
+UP_DI void mul_u32(u32 (&r)[N], const u32 (&a)[NA], u32 k) {
+    u64 c = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        u64 t = (u64)at(a, i) * k + c;
+        r[i] = (u32)t;
+        c = t >> 32;
+    }
+}
+
+// ----------------------------------------------------------- shifts
+// r = a << s (bits, dynamic s in [0, 32*N)), truncated to N limbs
+template <int N>
+UP_DI void shl_bits(u32 (&r)[N], const u32 (&a)[N], u32 s) {
+    u32 t[N];
+    copy_ext(t, a);
+    // limb shift by s/32, done as a barrel of static shifts
+    const u32 ls = s >> 5;
+#pragma unroll
+    for (int k = 1; k < N; k <<= 1) {
+        if (ls & (u32)k) {
+#pragma unroll
+            for (int i = N - 1; i >= 0; i--) t[i] = i >= k ? t[i >= k ? i - k : 0] : 0u;
+        }
+    }
+    const u32 bs = s & 31u;
+#pragma unroll
+    for (int i = N - 1; i >= 0; i--) r[i] = __funnelshift_l(i > 0 ? t[i > 0 ? i - 1 : 0] : 0u, t[i], bs);
+}
+
+// r = a >> s (bits, dynamic s in [0, 32*N))
+template <int N>
+UP_DI void shr_bits(u32 (&r)[N], const u32 (&a)[N], u32 s) {
+    u32 t[N];
+    copy_ext(t, a);
+    const u32 ls = s >> 5;
+#pragma unroll
+    for (int k = 1; k < N; k <<= 1) {
+        if (ls & (u32)k) {
+#pragma unroll
+            for (int i = 0; i < N; i++) t[i] = i + k < N ? t[i + k < N ? i + k : 0] : 0u;
+        }
+    }
+    const u32 bs = s & 31u;
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = __funnelshift_r(t[i], i + 1 < N ? t[i + 1 < N ? i + 1 : 0] : 0u, bs);
+}
+
+// ------------------------------------------------------------ division
+// Knuth, TAOCP vol. 2, 4.3.1, Algorithm D in base 2^32 with static array
+// sizes: the divisor is normalised to exactly NB limbs (top bit set) by a
+// dynamic left shift applied to both operands, so the quotient loop runs a
+// fixed NX+1 steps and every array stays in registers for small sizes.
+// q = floor(x / b), rem = x mod b.  Requires b != 0.
+template <int NX, int NB>
+UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&b)[NB]) {
+    if constexpr (NB == 1) {
+        const u32 d = b[0];
+        u64 r = 0;
+#pragma unroll
+        for (int i = NX - 1; i >= 0; i--) {
+            u64 cur = (r << 32) | x[i];
+            u64 qq = cur / d;
+            q[i] = (u32)qq;
+            r = cur - qq * d;
+        }
+        rem[0] = (u32)r;
+    } else {
+    constexpr int NU = NX + NB + 1;
+    const u32 bl = bitlen(b);
+    const u32 s = 32u * NB - bl;  // normalising shift
+    u32 bn[NB];
+    shl_bits(bn, b, s);
+    u32 un[NU];
+    {
+        u32 xe[NU];
+        copy_ext(xe, x);
+        shl_bits(un, xe, s);
+    }
+    const u32 vtop = bn[NB - 1];
+    const u32 vnext = bn[NB - 2];
+#pragma unroll(((NX + 1) * NB <= 96) ? NX + 1 : 1)
+    for (int j = NX; j >= 0; j--) {
+        const u64 num = ((u64)un[j + NB] << 32) | un[j + NB - 1];
+        u64 qhat = num / vtop;
+        u64 rhat = num - qhat * vtop;
+        while ((qhat >> 32) != 0u || qhat * vnext > ((rhat << 32) | un[j + NB - 2])) {
+            qhat--;
+            rhat += vtop;
+            if (rhat >> 32) break;
+        }
+        // multiply and subtract qhat * bn from un[j .. j+NB]
+        u64 carry = 0;
+        i64 borrow = 0;
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            u64 p = qhat * bn[i] + carry;
+            carry = p >> 32;
+            i64 t = (i64)un[i + j] - (i64)(u32)p - borrow;
+            un[i + j] = (u32)t;
+            borrow = t < 0 ? 1 : 0;
+        }
+        i64 t = (i64)un[j + NB] - (i64)carry - borrow;
+        un[j + NB] = (u32)t;
+        if (t < 0) {
+            qhat--;
+            u64 c = 0;
+#pragma unroll
+            for (int i = 0; i < NB; i++) {
+                c += (u64)un[i + j] + bn[i];
+                un[i + j] = (u32)c;
+                c >>= 32;
+            }
+            un[j + NB] += (u32)c;
+        }
+        if (j < NX) q[j] = (u32)qhat;
+    }
+    u32 rl[NB];
+#pragma unroll
+    for (int i = 0; i < NB; i++) rl[i] = un[i];
+    // the remainder (< bn) sits in un[0..NB); undo the normalising shift
+    shr_bits(rem, rl, s);
+    }
+}
+
+// Bit length of 10^k estimated the way the reference does before choosing
+// the 64-bit divide branch (AriesDecimal.hxx:799-804).
+__host__ __device__ constexpr u32 ref_shift_bits(u32 shift) {
+    return (shift / 3u) * 10u + (shift % 3u == 1u ? 4u : (shift % 3u == 2u ? 7u : 0u));
+}
+
+// Decimal divide with the reference's rule (DivOrMod, AriesDecimal.hxx:748-878):
+//   sign = sa ^ sb; dividend 0 -> +0; divisor 0 -> dividend unchanged + ERR_DIV0;
+//   shift = scale(b) + 4 (compile time: SHIFT);
+//   if bitlen(a) + ref_shift_bits(SHIFT) - 1 <= 64 and bitlen(b) <= 64:
+//       64-bit arithmetic: q = (a*10^SHIFT mod 2^64) / b, half-up with the
+//       doubled remainder taken mod 2^64                         (:581-596)
+//   else q = floor(a*10^SHIFT / b), half-up on 2*rem >= b, where a one-limb
+//       divisor doubles the remainder mod 2^32                   (:598-626, :862-873)
+// p10 holds the NP limbs of 10^SHIFT; P10W is 10^SHIFT mod 2^64.
+template <int NR, int NA, int NB, int NP, u32 SHIFT, u64 P10W>
+UP_DI u32 div_round(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32 (&b)[NB], u32 sb,
+                    const u32 (&p10)[NP]) {
+    sr = sa ^ sb;
+    if (is_zero(a)) {
+        zero(r);
+        sr = 0u;
+        return 0u;
+    }
+    if (is_zero(b)) {
+        copy_ext(r, a);
+        return ERR_DIV0;
+    }
+    const u32 hdt = bitlen(a);
+    const u32 hds = bitlen(b);
+    if (hdt + ref_shift_bits(SHIFT) - 1u <= 64u && hds <= 64u) {
+        const u64 dvs = ((u64)at(a, 0) | ((u64)at(a, 1) << 32)) * P10W;
+        const u64 dvt = (u64)at(b, 0) | ((u64)at(b, 1) << 32);
+        u64 q = dvs / dvt;
+        const u64 rm = dvs - q * dvt;
+        q += ((rm << 1) >= dvt) ? 1u : 0u;
+        zero(r);
+        r[0] = (u32)q;
+        if (NR > 1) r[NR > 1 ? 1 : 0] = (u32)(q >> 32);
+        return 0u;
+    }
+    constexpr int NX = NA + NP;
+    u32 x[NX];
+    mul(x, a, p10);
+    u32 q[NX];
+    u32 rem[NB];
+    divmod(q, rem, x, b);
+    bool up;
+    if (hds <= 32u) {
+        up = (u32)(rem[0] * 2u) >= b[0];
+    } else {
+        u32 dbl[NB + 1];
+        add(dbl, rem, rem);
+        up = cmp(dbl, b) >= 0;
+    }
+    copy_ext(r, q);
+    if (up) add_small(r, 1u);
+    return 0u;
+}
+
+// MOD with ModCalc rules (AriesDecimal.hxx:953-1012): raw magnitudes (no
+// alignment), scale 0, sign XOR, zero dividend -> +0.  A zero divisor is
+// undefined in the reference; here it yields 0 with ERR_DIV0.
+template <int NR, int NA, int NB>
+UP_DI u32 mod(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32 (&b)[NB], u32 sb) {
+    sr = sa ^ sb;
+    if (is_zero(a)) {
+        zero(r);
+        sr = 0u;
+        return 0u;
+    }
+    if (is_zero(b)) {
+        zero(r);
+        return ERR_DIV0;
+    }
+    u32 q[NA];
+    u32 rem[NB];
+    divmod(q, rem, a, b);
+    copy_ext(r, rem);
+    return 0u;
+}
+
+// Truncate toward zero by 10^K (RESCALE to a smaller scale).
+template <int NR, int NA, int NP>
+UP_DI void trunc_div_pow10(u32 (&r)[NR], const u32 (&a)[NA], const u32 (&p10)[NP]) {
+    u32 q[NA];
+    u32 rem[NP];
+    divmod(q, rem, a, p10);
+    copy_ext(r, q);
+}
+
+// Comparison with the reference rules: different signs decide by sign
+// alone (-0 < +0), else aligned magnitudes reversed for negatives.
+// op: 0 <, 1 <=, 2 >, 3 >=, 4 ==, 5 !=
+template <int NA, int NB>
+UP_DI u32 compare(int op, const u32 (&a)[NA], u32 sa, const u32 (&b)[NB], u32 sb) {
+    bool lt, gt, eq;
+    if (sa != sb) {
+        lt = sa == 1u;
+        gt = sa == 0u;
+        eq = false;
+    } else {
+        const int c = cmp(a, b);
+        eq = c == 0;
+        lt = sa == 0u ? c < 0 : c > 0;
+        gt = sa == 0u ? c > 0 : c < 0;
+    }
+    switch (op) {
+        case 0: return lt;
+        case 1: return !gt;
+        case 2: return gt;
+        case 3: return !lt;
+        case 4: return eq;
+        default: return !eq;
+    }
+}
+
+// ----------------------------------------------------- compact layout
+// Load a B-byte compact value from 4-byte-readable memory (shared-memory
+// tiles are padded so the word past the value is readable).
+template <int B, int N>
+UP_DI void ld_compact_words(const u8* p, u32 (&m)[N], u32& sign) {
+    static_assert(N * 4 >= B, "limbs too few for the compact width");
+    const unsigned long long addr = (unsigned long long)p;
+    const u32 off = (u32)(addr & 3u);
+    const u32* w = (const u32*)(p - off);
+    const u32 sh = off * 8u;
+    constexpr int W = (B + 3) / 4;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (i < W) {
+            const u32 lo = w[i];
+            const u32 hi = (off != 0u) ? w[i + 1] : 0u;
+            m[i] = __funnelshift_r(lo, hi, sh);
+        } else {
+            m[i] = 0u;
+        }
+    }
+    constexpr int TOPL = (B - 1) / 4;
+    constexpr int TOPB = ((B - 1) % 4) * 8 + 7;
+    sign = (m[TOPL] >> TOPB) & 1u;
+    m[TOPL] &= (TOPB == 31) ? 0x7fffffffu : ((1u << TOPB) - 1u);
+}
+
+// Byte-granular load (any alignment, never reads past the value).
+template <int B, int N>
+UP_DI void ld_compact_bytes(const u8* p, u32 (&m)[N], u32& sign) {
+    zero(m);
+#pragma unroll
+    for (int i = 0; i < B; i++) m[i / 4] |= (u32)p[i] << (8 * (i % 4));
+    constexpr int TOPL = (B - 1) / 4;
+    constexpr int TOPB = ((B - 1) % 4) * 8 + 7;
+    sign = (m[TOPL] >> TOPB) & 1u;
+    m[TOPL] &= (TOPB == 31) ? 0x7fffffffu : ((1u << TOPB) - 1u);
+}
+
+// Overflow test: any magnitude bit at or above 8*B-1 would be lost or would
+// collide with the sign bit.
+template <int B, int N>
+UP_DI u32 compact_overflow(const u32 (&m)[N]) {
+    constexpr int BIT = 8 * B - 1;
+    u32 o = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (32 * i + 32 <= BIT) continue;
+        const u32 mask = (32 * i >= BIT) ? 0xffffffffu : ~((1u << (BIT - 32 * i)) - 1u);
+        o |= m[i] & mask;
+    }
+    return o ? ERR_OVERFLOW : 0u;
+}
+
+// Store with ToCompactDecimal + SET_SIGN_BIT: low B bytes, then the sign
+// OR-ed into bit 7 of the last byte.  Byte stores (any alignment).
+template <int B, int N>
+UP_DI u32 st_compact_bytes(u8* p, const u32 (&m)[N], u32 sign) {
+#pragma unroll
+    for (int i = 0; i < B; i++) {
+        u32 byte = (at(m, i / 4) >> (8 * (i % 4))) & 0xffu;
+        if (i == B - 1) byte |= sign << 7;
+        p[i] = (u8)byte;
+    }
+    return compact_overflow<B>(m);
+}
+
+// Same, 4-byte aligned p and B % 4 == 0: word stores.
+template <int B, int N>
+UP_DI u32 st_compact_words(u8* p, const u32 (&m)[N], u32 sign) {
+    static_assert(B % 4 == 0, "word store needs B % 4 == 0");
+    u32* w = (u32*)p;
+#pragma unroll
+    for (int i = 0; i < B / 4; i++) {
+        u32 v = at(m, i);
+        if (i == B / 4 - 1) v |= sign << 31;
+        w[i] = v;
+    }
+    return compact_overflow<B>(m);
+}
+
+// ------------------------------------------------------ column access
+// Per-column kernel argument: the AriesColumnDataIterator shape
+// (AriesColumnDataIterator.hxx:8-41).
+struct KCol {
+    const u8* data;
+    const u8* const* blocks;
+    const i64* prefix;
+    const int* indices;
+    int n_blocks;
+    int value_bytes;
+};
+
+// Row -> value pointer for the block/indirection path
+// (AriesColumnDataIterator::operator[], AriesColumnDataIterator.cu:60-115).
+// Returns nullptr for a NULL index.
+UP_DI const u8* col_ptr(const KCol& c, i64 row) {
+    i64 r = row;
+    if (c.indices) {
+        const int j = c.indices[row];
+        if (j < 0) return nullptr;
+        r = j;
+    }
+    if (c.n_blocks == 0) return c.data + r * (i64)c.value_bytes;
+    int lo = 0, hi = c.n_blocks;  // upper-bound search over prefix[0..n_blocks]
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (c.prefix[mid] <= r) lo = mid + 1;
+        else hi = mid;
+    }
+    const int blk = lo - 1;
+    return c.blocks[blk] + (r - c.prefix[blk]) * (i64)c.value_bytes;
+}
+
+// ------------------------------------------------- tile staging helpers
+// Cooperative copy of n bytes global -> shared.  16-byte vectors when both
+// ends allow it, bytes otherwise.
+UP_DI void tile_copy_in(u8* __restrict__ dst, const u8* __restrict__ src, int n, bool vec_ok) {
+    if (vec_ok && (n & 15) == 0) {
+        const uint4* s = (const uint4*)src;
+        uint4* d = (uint4*)dst;
+        for (int i = threadIdx.x; i < (n >> 4); i += blockDim.x) d[i] = s[i];
+    } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+    }
+}
+
+UP_DI void tile_copy_out(u8* __restrict__ dst, const u8* __restrict__ src, int n, bool vec_ok) {
+    if (vec_ok && (n & 15) == 0) {
+        const uint4* s = (const uint4*)src;
+        uint4* d = (uint4*)dst;
+        for (int i = threadIdx.x; i < (n >> 4); i += blockDim.x) d[i] = s[i];
+    } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+    }
+}
+
+// ------------------------------------------- exact group accumulators
+// Two's complement accumulation of a sign-magnitude value into NACC limbs in
+// memory with 32-bit atomics, carries propagated limb by limb.  Exact as long
+// as the true sum fits NACC limbs signed (the host sizes NACC for that).
+template <int NACC, int N>
+UP_DI void atomic_acc_add(u32* acc, const u32 (&m)[N], u32 sign) {
+    u32 t[NACC];
+    copy_ext(t, m);
+    if (sign) negate(t);
+    u32 carry = 0;
+#pragma unroll
+    for (int i = 0; i < NACC; i++) {
+        const u32 v = t[i];
+        u32 add = v + carry;
+        u32 c1 = (add < v) ? 1u : 0u;  // v + carry wrapped
+        if (add != 0u) {
+            const u32 old = atomicAdd(acc + i, add);
+            c1 |= (old + add < old) ? 1u : 0u;
+        }
+        carry = c1;
+    }
+}
+
+// The reference's nullable_type<Decimal> image of a SUM/AVG result
+// (decimal.hxx:130-140 plus the leading flag; kernel_segreduce.hxx:609-612):
+// [0] flag, [1] sign, [2] prec, [3] frac, [4] error, [5..133) v[32] LE.
+// prec and error are left 0 (the reference leaves them unwritten).
+template <int N>
+UP_DI void agg_image(u8* img, u32 flag, u32 sign, u32 frac, const u32 (&m)[N]) {
+    img[0] = (u8)flag;
+    img[1] = (u8)sign;
+    img[2] = 0;
+    img[3] = (u8)frac;
+    img[4] = 0;
+#pragma unroll 4
+    for (int i = 0; i < 32; i++) {
+        const u32 w = i < N ? m[i < N ? i : 0] : 0u;
+        img[5 + 4 * i] = (u8)w;
+        img[6 + 4 * i] = (u8)(w >> 8);
+        img[7 + 4 * i] = (u8)(w >> 16);
+        img[8 + 4 * i] = (u8)(w >> 24);
+    }
+}
+
+}  // namespace up
+
+#endif  // UP_DEV_CUH_

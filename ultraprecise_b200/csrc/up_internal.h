@@ -1,0 +1,102 @@
+// up_internal.h — host-side internals shared by the C++ sources of
+// libultraprecise.so (not part of the public ABI).
+#ifndef UP_INTERNAL_H_
+#define UP_INTERNAL_H_
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ultraprecise.h"
+
+namespace upi {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+up_status fail(up_status s, const std::string& msg);
+const char* last_error();
+
+// ---------------------------------------------------------------- tables
+int compact_bytes(int precision);    // B(p) with the extension rule
+int precision_words(int precision);  // W(p) with the extension rule
+constexpr int kMaxPrecision = 4000;
+
+// ------------------------------------------------------- host big integer
+// Little-endian base-2^32 magnitude, trimmed (no leading zero limbs).
+struct Big {
+    std::vector<uint32_t> m;
+    bool is_zero() const { return m.empty(); }
+};
+void big_trim(Big& a);
+Big big_from_u64(uint64_t v);
+Big big_pow10(int k);
+Big big_mul(const Big& a, const Big& b);
+Big big_add(const Big& a, const Big& b);
+Big big_sub(const Big& a, const Big& b);  // a >= b
+int big_cmp(const Big& a, const Big& b);
+int big_bitlen(const Big& a);
+Big big_divmod_small(const Big& a, uint32_t d, uint32_t* rem);
+uint64_t big_low64(const Big& a);  // a mod 2^64
+std::string big_to_dec(const Big& a);
+Big big_from_dec(const std::string& s);
+
+// ------------------------------------------------------ expression typing
+// Per-node facts the code generator needs: the evaluation scale (static),
+// an upper bound on magnitude bits, hence the limb count.
+struct NodeFacts {
+    int scale = 0;
+    int bits = 1;
+    int limbs = 1;
+    bool is_compare = false;
+};
+up_status analyze_nodes(const up_expr_node* nodes, int n_nodes, const up_col_type* cols, int n_cols,
+                        std::vector<NodeFacts>& facts, std::vector<int>& topo, const std::vector<int>& roots);
+int limbs_for_bits(int bits);
+
+// ------------------------------------------------------------ code generation
+struct GeneratedModule {
+    std::string source;
+    std::vector<std::string> kernels;
+    // expression modules
+    int out_precision = 0, out_scale = 0, out_bytes = 0;
+    bool out_is_compare = false;
+    int block_threads = 256;
+    int tile_rows = 256;
+    int smem_bytes = 0;
+    std::vector<int> in_bytes;  // per referenced input column: value bytes
+    // query modules
+    int n_aggs = 0;
+    std::vector<int> agg_kind, agg_scale, agg_acc_limbs, agg_acc_offset;
+    int acc_words_per_group = 0;  // sum over aggregates (count excluded)
+};
+up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
+                               int n_cols, const up_compile_opts* opts, GeneratedModule& out);
+up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up_col_type* cols, int n_cols,
+                                const up_query_agg* aggs, int n_aggs, const up_compile_opts* opts,
+                                GeneratedModule& out);
+
+// ------------------------------------------------------------------ JIT
+struct JitKernelSet;  // opaque: loaded library + kernel handles
+struct JitModule {
+    std::shared_ptr<JitKernelSet> ks;
+    GeneratedModule gen;
+};
+// Compile (or fetch from the cache) and load.  Thread-safe.
+up_status jit_compile_cubin(const std::string& src, std::vector<char>& cubin);
+up_status jit_get(const GeneratedModule& gen, std::shared_ptr<JitKernelSet>& out);
+void* jit_kernel(const JitKernelSet& ks, const std::string& name);  // cudaKernel_t as void*
+int jit_cache_size(bool clear);
+const std::string& device_header_source();
+
+// ------------------------------------------------------------ devices
+int sm_count_current();
+
+}  // namespace upi
+
+struct up_module {
+    upi::JitModule jm;
+    bool is_query = false;
+};
+
+#endif  // UP_INTERNAL_H_

@@ -1,0 +1,253 @@
+// up_jit.cpp — NVRTC compile to CUBIN for sm_100a, module cache, loading.
+//
+// Replaces the reference's AriesDynamicKernelManager (DynamicKernel.h:50-117,
+// DynamicKernel.cu:10-158): there, NVRTC produced PTX for compute_XY, which
+// was linked with libariesdatatype.a and loaded on every device, with an LRU
+// of 100 modules keyed by the full source.  Here NVRTC emits a CUBIN for
+// sm_100a directly (the device arithmetic is a header compiled into each
+// kernel, so there is no link step), the cubin is cached in memory (LRU keyed
+// by the source) and on disk, and it is loaded once with the runtime's
+// context-independent cudaLibraryLoadData, whose kernel handles are valid on
+// every device of the process.
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+#include <dlfcn.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <list>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <unordered_map>
+
+#include "up_internal.h"
+
+namespace upi {
+
+#include "up_dev_embed.inc"  // defines kUpDevCuh (the text of up_dev.cuh)
+
+const std::string& device_header_source() {
+    static const std::string s(kUpDevCuh);
+    return s;
+}
+
+struct JitKernelSet {
+    std::vector<char> cubin;
+    cudaLibrary_t lib = nullptr;
+    std::map<std::string, cudaKernel_t> kernels;
+    ~JitKernelSet() {
+        if (lib) cudaLibraryUnload(lib);
+    }
+};
+
+namespace {
+
+uint64_t fnv1a(const std::string& s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+const char* kArch = "--gpu-architecture=sm_100a";
+
+// Default: <package>/_jitcache beside <package>/_lib/libultraprecise.so, so
+// cubins compiled at build time travel with the library; UP_JIT_CACHE_DIR
+// overrides it.
+std::string cache_dir() {
+    const char* d = getenv("UP_JIT_CACHE_DIR");
+    if (d && *d) return d;
+    Dl_info info;
+    if (dladdr((void*)&cache_dir, &info) && info.dli_fname) {
+        std::string p = info.dli_fname;
+        size_t k = p.rfind('/');
+        if (k != std::string::npos) {
+            std::string libdir = p.substr(0, k);
+            size_t k2 = libdir.rfind('/');
+            if (k2 != std::string::npos) return libdir.substr(0, k2) + "/_jitcache";
+        }
+    }
+    const char* home = getenv("HOME");
+    return std::string(home && *home ? home : "/tmp") + "/.cache/ultraprecise_b200";
+}
+
+bool disk_cache_enabled() {
+    const char* e = getenv("UP_JIT_DISK_CACHE");
+    return !(e && e[0] == '0');
+}
+
+void mkdirs(const std::string& path) {
+    std::string cur;
+    std::stringstream ss(path);
+    std::string part;
+    if (!path.empty() && path[0] == '/') cur = "/";
+    while (std::getline(ss, part, '/')) {
+        if (part.empty()) continue;
+        cur += part + "/";
+        mkdir(cur.c_str(), 0755);
+    }
+}
+
+std::string full_key(const std::string& src) {
+    int maj = 0, min = 0;
+    nvrtcVersion(&maj, &min);
+    return std::string(kArch) + "|nvrtc" + std::to_string(maj) + "." + std::to_string(min) + "|" + src;
+}
+
+bool read_file(const std::string& p, std::string& out) {
+    std::ifstream f(p, std::ios::binary);
+    if (!f) return false;
+    std::ostringstream o;
+    o << f.rdbuf();
+    out = o.str();
+    return true;
+}
+
+void write_file_atomic(const std::string& p, const std::string& data) {
+    std::string tmp = p + ".tmp." + std::to_string(getpid());
+    {
+        std::ofstream f(tmp, std::ios::binary);
+        if (!f) return;
+        f.write(data.data(), (std::streamsize)data.size());
+    }
+    rename(tmp.c_str(), p.c_str());
+}
+
+up_status nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::string& log) {
+    nvrtcProgram prog;
+    const char* hdr_src[1] = {device_header_source().c_str()};
+    const char* hdr_name[1] = {"up_dev.cuh"};
+    nvrtcResult r = nvrtcCreateProgram(&prog, src.c_str(), "up_kernel.cu", 1, hdr_src, hdr_name);
+    if (r != NVRTC_SUCCESS) return fail(UP_ERR_COMPILE, std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r));
+    const char* opts[] = {kArch, "-std=c++17", "-lineinfo", "--restrict", "-DUP_NVRTC=1"};
+    r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+    size_t ls = 0;
+    nvrtcGetProgramLogSize(prog, &ls);
+    log.assign(ls, '\0');
+    if (ls) nvrtcGetProgramLog(prog, &log[0]);
+    if (r != NVRTC_SUCCESS) {
+        nvrtcDestroyProgram(&prog);
+        return fail(UP_ERR_COMPILE, "NVRTC: " + std::string(nvrtcGetErrorString(r)) + "\n" + log);
+    }
+    size_t n = 0;
+    r = nvrtcGetCUBINSize(prog, &n);
+    if (r != NVRTC_SUCCESS || n == 0) {
+        nvrtcDestroyProgram(&prog);
+        return fail(UP_ERR_COMPILE, "NVRTC produced no CUBIN");
+    }
+    cubin.resize(n);
+    nvrtcGetCUBIN(prog, cubin.data());
+    nvrtcDestroyProgram(&prog);
+    return UP_OK;
+}
+
+struct Cache {
+    std::mutex mu;
+    std::list<std::string> lru;  // most recent at front
+    std::unordered_map<std::string, std::pair<std::shared_ptr<JitKernelSet>, std::list<std::string>::iterator>> map;
+    size_t cap = 256;
+};
+
+Cache& cache() {
+    static Cache* c = new Cache();  // intentionally leaked: outlives static destructors
+    return *c;
+}
+
+}  // namespace
+
+up_status jit_compile_cubin(const std::string& src, std::vector<char>& cubin) {
+    const std::string key = full_key(src);
+    const uint64_t h = fnv1a(key);
+    char name[32];
+    snprintf(name, sizeof name, "%016llx", (unsigned long long)h);
+    std::string dir = cache_dir();
+    std::string base = dir + "/" + name;
+    if (disk_cache_enabled()) {
+        std::string k2, bin;
+        if (read_file(base + ".key", k2) && k2 == key && read_file(base + ".cubin", bin) && !bin.empty()) {
+            cubin.assign(bin.begin(), bin.end());
+            return UP_OK;
+        }
+    }
+    std::string log;
+    up_status st = nvrtc_compile(src, cubin, log);
+    if (st != UP_OK) return st;
+    if (disk_cache_enabled()) {
+        mkdirs(dir);
+        write_file_atomic(base + ".cubin", std::string(cubin.begin(), cubin.end()));
+        write_file_atomic(base + ".key", key);
+    }
+    return UP_OK;
+}
+
+up_status jit_get(const GeneratedModule& gen, std::shared_ptr<JitKernelSet>& out) {
+    Cache& c = cache();
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        auto it = c.map.find(gen.source);
+        if (it != c.map.end()) {
+            c.lru.erase(it->second.second);
+            c.lru.push_front(gen.source);
+            it->second.second = c.lru.begin();
+            out = it->second.first;
+            return UP_OK;
+        }
+    }
+    auto ks = std::make_shared<JitKernelSet>();
+    up_status st = jit_compile_cubin(gen.source, ks->cubin);
+    if (st != UP_OK) return st;
+    cudaError_t e = cudaLibraryLoadData(&ks->lib, ks->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e != cudaSuccess) {
+        ks->lib = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? UP_ERR_NO_DEVICE : UP_ERR_CUDA,
+                    std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e));
+    }
+    for (const auto& k : gen.kernels) {
+        cudaKernel_t h = nullptr;
+        e = cudaLibraryGetKernel(&h, ks->lib, k.c_str());
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(UP_ERR_CUDA, "cudaLibraryGetKernel(" + k + "): " + cudaGetErrorString(e));
+        }
+        ks->kernels[k] = h;
+    }
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.map.find(gen.source);
+    if (it != c.map.end()) {  // another thread won the race
+        out = it->second.first;
+        return UP_OK;
+    }
+    c.lru.push_front(gen.source);
+    c.map[gen.source] = {ks, c.lru.begin()};
+    while (c.map.size() > c.cap) {
+        c.map.erase(c.lru.back());
+        c.lru.pop_back();
+    }
+    out = ks;
+    return UP_OK;
+}
+
+void* jit_kernel(const JitKernelSet& ks, const std::string& name) {
+    auto it = ks.kernels.find(name);
+    return it == ks.kernels.end() ? nullptr : (void*)it->second;
+}
+
+int jit_cache_size(bool clear) {
+    Cache& c = cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    int n = (int)c.map.size();
+    if (clear) {
+        c.map.clear();
+        c.lru.clear();
+    }
+    return n;
+}
+
+}  // namespace upi

@@ -1,0 +1,338 @@
+// up_kernels.cu — precompiled sm_100a kernels: segment ids, AVG division,
+// small-key grouping, and the benchmark utilities of ultraprecise_util.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+
+#include "../../include/ultraprecise.h"
+#include "../../include/ultraprecise_util.h"
+#include "up_dev.cuh"
+#include "up_internal.h"
+#include "up_kernels.h"
+
+namespace upi {
+
+using up::u32;
+using up::u64;
+using up::u8;
+
+// ------------------------------------------------ segment starts -> ids
+// group of row position i = (last start <= i); the reference's segments
+// (AriesSqlOperator_group.cu:14-54) are ascending starts into `associated`.
+__global__ void k_fill_segment_gids(const int32_t* __restrict__ starts, int32_t n_groups, int64_t rows,
+                                    int32_t* __restrict__ gid) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) {
+        int lo = 0, hi = n_groups;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if ((int64_t)starts[mid] <= i) lo = mid + 1;
+            else hi = mid;
+        }
+        gid[i] = lo - 1;
+    }
+}
+
+cudaError_t launch_fill_segment_gids(const int32_t* starts, int32_t n_groups, int64_t rows, int32_t* gid,
+                                     cudaStream_t s) {
+    if (rows <= 0) return cudaSuccess;
+    int64_t blocks = std::min<int64_t>((rows + 255) / 256, 148 * 16);
+    k_fill_segment_gids<<<(unsigned)blocks, 256, 0, s>>>(starts, n_groups, rows, gid);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------ AVG division
+// DivisionInt64 (AriesSqlOperator_helpers.cu:717-763 -> do_div,
+// kernel_util.hxx:426-438): Decimal(sum) /= int64 count, i.e. the divide
+// rule with the divisor a scale-0 integer: scale + 4, half-up.
+__global__ void k_division_int64(const u8* __restrict__ sums, const int64_t* __restrict__ counts, int32_t n,
+                                 u8* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u8* img = sums + (int64_t)i * UP_AGG_DECIMAL_BYTES;
+    u32 m[32];
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+        m[k] = (u32)img[5 + 4 * k] | ((u32)img[6 + 4 * k] << 8) | ((u32)img[7 + 4 * k] << 16) |
+               ((u32)img[8 + 4 * k] << 24);
+    const u32 sign = img[1] ? 1u : 0u;
+    const u64 cnt = (u64)counts[i];
+    const u32 c2[2] = {(u32)cnt, (u32)(cnt >> 32)};
+    const u32 p10[1] = {10000u};
+    u32 q[34];
+    u32 sq;
+    const u32 err = up::div_round<34, 32, 2, 1, 4u, 10000ull>(q, sq, m, sign, c2, 0u, p10);
+    u8* o = out + (int64_t)i * UP_AGG_DECIMAL_BYTES;
+    up::agg_image(o, img[0], sq, (u32)img[3] + 4u, q);
+    o[4] = (err & up::ERR_DIV0) ? 2 : 0;  // Decimal::error = ERR_DIV_BY_ZERO (decimal.hxx:28)
+}
+
+cudaError_t launch_division_int64(const uint8_t* sums, const int64_t* counts, int32_t n, uint8_t* out,
+                                  cudaStream_t s) {
+    k_division_int64<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(sums, counts, n, out);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------- small-key grouping
+struct KeyCols {
+    const u8* col[4];
+    int bytes[4];
+    int n;
+};
+
+__device__ __forceinline__ u32 row_key(const KeyCols& k, int64_t row) {
+    u32 key = 0;
+    for (int c = 0; c < k.n; c++)
+        for (int b = 0; b < k.bytes[c]; b++) key = (key << 8) | k.col[c][row * k.bytes[c] + b];
+    return key;
+}
+
+__global__ void k_mark_keys(KeyCols k, int64_t rows, u32* __restrict__ flags) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) {
+        const u32 key = row_key(k, i);
+        if (flags[key] == 0u) flags[key] = 1u;
+    }
+}
+
+// one block: exclusive scan of 65536 presence flags -> dense ids in key order
+__global__ void __launch_bounds__(1024) k_scan_keys(const u32* __restrict__ flags, int32_t* __restrict__ ids,
+                                                    int32_t* __restrict__ n_out, u8* __restrict__ keys_out,
+                                                    int key_bytes) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x;
+    const int per = 65536 / 1024;
+    int c = 0;
+    for (int j = 0; j < per; j++) c += flags[t * per + j] ? 1 : 0;
+    part[t] = c;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        int v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int base = part[t] - c;
+    for (int j = 0; j < per; j++) {
+        const int key = t * per + j;
+        if (flags[key]) {
+            ids[key] = base;
+            if (keys_out) {
+                for (int b = 0; b < key_bytes; b++) keys_out[(int64_t)base * key_bytes + b] =
+                    (u8)(key >> (8 * (key_bytes - 1 - b)));
+            }
+            base++;
+        } else {
+            ids[key] = -1;
+        }
+    }
+    if (t == 1023) *n_out = part[1023];
+}
+
+__global__ void k_map_keys(KeyCols k, int64_t rows, const int32_t* __restrict__ ids, int32_t* __restrict__ gid) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) gid[i] = ids[row_key(k, i)];
+}
+
+cudaError_t launch_group_ids_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                        int64_t rows, int32_t* gid, int32_t* n_groups, void* group_keys,
+                                        cudaStream_t s) {
+    KeyCols k;
+    int total = 0;
+    for (int c = 0; c < 4; c++) {
+        k.col[c] = c < n_keys ? (const u8*)key_cols[c] : nullptr;
+        k.bytes[c] = c < n_keys ? key_bytes[c] : 0;
+        total += k.bytes[c];
+    }
+    k.n = n_keys;
+    void* scratch = nullptr;
+    cudaError_t e = cudaMallocAsync(&scratch, 65536 * 8 + 16, s);
+    if (e != cudaSuccess) return e;
+    u32* flags = (u32*)scratch;
+    int32_t* ids = (int32_t*)((u8*)scratch + 65536 * 4);
+    int32_t* dn = (int32_t*)((u8*)scratch + 65536 * 8);
+    e = cudaMemsetAsync(flags, 0, 65536 * 4, s);
+    int64_t blocks = std::min<int64_t>((rows + 255) / 256, 148 * 8);
+    if (e == cudaSuccess && rows > 0) {
+        k_mark_keys<<<(unsigned)blocks, 256, 0, s>>>(k, rows, flags);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        k_scan_keys<<<1, 1024, 0, s>>>(flags, ids, dn, (u8*)group_keys, total);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && rows > 0) {
+        k_map_keys<<<(unsigned)blocks, 256, 0, s>>>(k, rows, ids, gid);
+        e = cudaGetLastError();
+    }
+    int32_t hn = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hn, dn, 4, cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) *n_groups = hn;
+    return e;
+}
+
+// ---------------------------------------------------------- utilities
+__device__ __forceinline__ u64 splitmix64(u64 x) {
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+constexpr int kGenMaxLimbs = 160;  // p up to ~1500 digits
+
+__global__ void k_gen_digits(u8* __restrict__ out, int64_t rows, int p, int bytes, u64 seed, int signed_,
+                             int nonzero) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int L = (bytes + 3) / 4;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += stride) {
+        u32 m[kGenMaxLimbs];
+        u64 st = seed ^ ((u64)row * 0xd1b54a32d192ed03ull);
+        u32 sign = 0;
+        for (int attempt = 0; attempt < 64; attempt++) {
+            for (int i = 0; i < L; i++) m[i] = 0;
+            int left = p;
+            bool nz = false;
+            while (left > 0) {
+                const int d = left >= 9 ? 9 : left;
+                left -= d;
+                u32 pw = 1;
+                for (int j = 0; j < d; j++) pw *= 10u;
+                st = splitmix64(st);
+                const u32 chunk = (u32)(((unsigned __int128)st * pw) >> 64);
+                nz |= chunk != 0;
+                u64 c = chunk;
+                for (int i = 0; i < L; i++) {
+                    u64 t = (u64)m[i] * pw + c;
+                    m[i] = (u32)t;
+                    c = t >> 32;
+                }
+            }
+            st = splitmix64(st);
+            sign = signed_ ? (u32)(st >> 63) : 0u;
+            if (!nonzero || nz) break;
+        }
+        u8* o = out + row * bytes;
+        for (int i = 0; i < bytes; i++) o[i] = (u8)(m[i / 4] >> (8 * (i % 4)));
+        o[bytes - 1] |= (u8)(sign << 7);
+    }
+}
+
+__global__ void k_gen_range(u8* __restrict__ out, int64_t rows, int bytes, long long lo, u64 n, long long step,
+                            u64 seed) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows; row += stride) {
+        const u64 r = splitmix64(seed ^ ((u64)row * 0xd1b54a32d192ed03ull));
+        const u64 idx = (u64)(((unsigned __int128)r * n) >> 64);
+        const long long v = lo + (long long)idx * step;
+        const u64 mag = v < 0 ? (u64)(-(v + 1)) + 1u : (u64)v;
+        u8* o = out + row * bytes;
+        for (int i = 0; i < bytes; i++) o[i] = i < 8 ? (u8)(mag >> (8 * i)) : 0;
+        o[bytes - 1] |= (u8)((v < 0 ? 1u : 0u) << 7);
+    }
+}
+
+__global__ void k_flush(uint4* __restrict__ buf, int64_t n, u32 salt) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        buf[i] = make_uint4(salt, (u32)i, salt ^ 1u, (u32)(i >> 32));
+}
+
+// Independent 32x32+64 multiply-adds: 8 chains per thread, no dependency
+// between chains, one dependency per chain per iteration.
+__global__ void __launch_bounds__(256) k_imad(u64* __restrict__ sink, int iters, u32 seed) {
+    u32 x[8];
+    u64 acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        x[k] = seed * (threadIdx.x + 1u) + 977u * k;
+        acc[k] = k;
+    }
+    const u32 y = seed ^ 0x9e3779b9u;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[k] = (u64)x[k] * y + acc[k];
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] ^= (u32)acc[k];
+    }
+    u64 s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s ^= acc[k];
+    if (s == 0x123456789ull) sink[0] = s;
+}
+
+}  // namespace upi
+
+using namespace upi;
+
+extern "C" {
+
+up_status up_util_gen_digits(void* out, int64_t rows, int32_t precision, uint64_t seed, int32_t signed_,
+                             int32_t nonzero, void* stream) {
+    const int b = compact_bytes(precision);
+    if (b < 1 || (b + 3) / 4 > kGenMaxLimbs) return fail(UP_ERR_INVALID_ARG, "precision out of generator range");
+    if (rows < 0 || (rows > 0 && !out)) return fail(UP_ERR_INVALID_ARG, "bad output");
+    if (rows == 0) return UP_OK;
+    int64_t blocks = std::min<int64_t>((rows + 127) / 128, 148 * 16);
+    k_gen_digits<<<(unsigned)blocks, 128, 0, (cudaStream_t)stream>>>((u8*)out, rows, precision, b, seed, signed_,
+                                                                      nonzero);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? UP_OK : fail(UP_ERR_CUDA, cudaGetErrorString(e));
+}
+
+up_status up_util_gen_range(void* out, int64_t rows, int32_t precision, int64_t lo, int64_t hi, int64_t step,
+                            uint64_t seed, void* stream) {
+    const int b = compact_bytes(precision);
+    if (b < 1 || step <= 0 || hi < lo) return fail(UP_ERR_INVALID_ARG, "bad range");
+    if (rows < 0 || (rows > 0 && !out)) return fail(UP_ERR_INVALID_ARG, "bad output");
+    if (rows == 0) return UP_OK;
+    const u64 n = (u64)((hi - lo) / step) + 1u;
+    int64_t blocks = std::min<int64_t>((rows + 255) / 256, 148 * 16);
+    k_gen_range<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>((u8*)out, rows, b, lo, n, step, seed);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? UP_OK : fail(UP_ERR_CUDA, cudaGetErrorString(e));
+}
+
+up_status up_util_flush_l2(void* buf, int64_t bytes, void* stream) {
+    if (!buf || bytes < 16) return fail(UP_ERR_INVALID_ARG, "bad buffer");
+    static u32 salt = 1;
+    k_flush<<<148 * 4, 256, 0, (cudaStream_t)stream>>>((uint4*)buf, bytes / 16, salt++);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? UP_OK : fail(UP_ERR_CUDA, cudaGetErrorString(e));
+}
+
+up_status up_util_imad_peak(double* madds_per_s, void* stream) {
+    if (!madds_per_s) return fail(UP_ERR_INVALID_ARG, "NULL result");
+    cudaStream_t s = (cudaStream_t)stream;
+    int sms = sm_count_current();
+    if (sms <= 0) return fail(UP_ERR_NO_DEVICE, "no CUDA device");
+    u64* sink = nullptr;
+    if (cudaMallocAsync((void**)&sink, 8, s) != cudaSuccess) return fail(UP_ERR_NO_MEMORY, "sink");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    k_imad<<<blocks, threads, 0, s>>>(sink, 64, 7u);  // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; rep++) {
+        cudaEventRecord(a, s);
+        k_imad<<<blocks, threads, 0, s>>>(sink, iters, 11u + rep);
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFreeAsync(sink, s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(UP_ERR_CUDA, cudaGetErrorString(e));
+    *madds_per_s = (double)blocks * threads * 8.0 * iters / (best * 1e-3);
+    return UP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+"""Device-side runtime over the C ABI.
+
+torch is used only for device memory and streams; every computation runs in
+libultraprecise.so's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Sequence
+
+import torch
+
+from . import abi, codec
+from .expr import Built, ColType, Expr, build, derive_types
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+@dataclass
+class DeviceColumn:
+    """A compact decimal column in HBM: rows x value_bytes uint8."""
+    data: torch.Tensor
+    precision: int
+    scale: int
+    nullable: bool = False
+    indices: torch.Tensor | None = None   # int32 row indirection (-1 = NULL)
+
+    @property
+    def value_bytes(self) -> int:
+        return codec.compact_bytes(self.precision) + (1 if self.nullable else 0)
+
+    @property
+    def rows(self) -> int:
+        if self.indices is not None:
+            return self.indices.numel()
+        return self.data.numel() // self.value_bytes
+
+    def up_column(self) -> abi.UpColumn:
+        c = abi.UpColumn()
+        c.data = self.data.data_ptr()
+        c.blocks = None
+        c.block_prefix = None
+        c.n_blocks = 0
+        c.indices = self.indices.data_ptr() if self.indices is not None else None
+        c.precision = self.precision
+        c.scale = self.scale
+        c.value_bytes = self.value_bytes
+        c.nullable = 1 if self.nullable else 0
+        return c
+
+    @staticmethod
+    def from_host(raw: bytes, precision: int, scale: int, device="cuda", nullable=False) -> "DeviceColumn":
+        t = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(device) if raw else torch.empty(
+            0, dtype=torch.uint8, device=device)
+        return DeviceColumn(t, precision, scale, nullable)
+
+    def col_type(self) -> ColType:
+        return ColType(self.precision, self.scale, self.nullable)
+
+
+def _columns_array(cols: Sequence[DeviceColumn]):
+    arr = (abi.UpColumn * max(1, len(cols)))()
+    for i, c in enumerate(cols):
+        arr[i] = c.up_column()
+    return arr
+
+
+class ExprModule:
+    """A compiled projection kernel (the reference's AEExprCalcNode kernel)."""
+
+    def __init__(self, built: Built, root: int, threads_per_value: int = 0, block_threads: int = 0):
+        lib = abi.load()
+        self.built = built
+        self.root = root
+        opts = abi.UpCompileOpts(threads_per_value, block_threads, 0)
+        h = C.c_void_p()
+        abi.check(lib.up_module_compile(built.nodes, built.n_nodes, root, built.col_types, built.n_cols,
+                                        C.byref(opts), C.byref(h)), "up_module_compile")
+        self._h = h
+        p, s, vb = C.c_int32(), C.c_int32(), C.c_int32()
+        abi.check(lib.up_module_result_type(h, C.byref(p), C.byref(s), C.byref(vb)), "up_module_result_type")
+        self.precision, self.scale, self.value_bytes = p.value, s.value, vb.value
+
+    def source(self) -> str:
+        lib = abi.load()
+        n = lib.up_module_source(self._h, None, 0)
+        buf = C.create_string_buffer(int(n) + 1)
+        lib.up_module_source(self._h, buf, n + 1)
+        return buf.value.decode()
+
+    def launch(self, cols: Sequence[DeviceColumn], rows: int | None = None, out: torch.Tensor | None = None,
+               err: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        lib = abi.load()
+        if rows is None:
+            rows = cols[0].rows if cols else 0
+        if out is None:
+            out = torch.empty(rows * self.value_bytes, dtype=torch.uint8, device="cuda")
+        arr = _columns_array(cols)
+        abi.check(lib.up_expr_launch(self._h, arr, len(cols), rows, out.data_ptr(),
+                                     err.data_ptr() if err is not None else None, _stream_ptr(stream)),
+                  "up_expr_launch")
+        return out
+
+    def __del__(self):
+        try:
+            abi.load().up_module_release(self._h)
+        except Exception:
+            pass
+
+
+def compile_expr(root: Expr, cols: Sequence[ColType], **kw) -> ExprModule:
+    b = build([root], cols)
+    derive_types(b)
+    return ExprModule(b, b.roots[0], **kw)
+
+
+class QueryModule:
+    """A compiled fused expression + grouped aggregate kernel pair."""
+
+    def __init__(self, built: Built, aggs: Sequence[tuple[int, int]]):
+        lib = abi.load()
+        self.built = built
+        self.aggs = list(aggs)
+        qa = (abi.UpQueryAgg * len(aggs))()
+        for i, (k, r) in enumerate(aggs):
+            qa[i].kind = k
+            qa[i].root = r
+        h = C.c_void_p()
+        abi.check(lib.up_query_compile(built.nodes, built.n_nodes, built.col_types, built.n_cols, qa, len(aggs),
+                                       None, C.byref(h)), "up_query_compile")
+        self._h = h
+
+    def launch(self, cols: Sequence[DeviceColumn], group_ids: torch.Tensor, n_groups: int,
+               outs: Sequence[torch.Tensor] | None = None, err: torch.Tensor | None = None,
+               stream=None, rows: int | None = None) -> list[torch.Tensor]:
+        lib = abi.load()
+        if rows is None:
+            rows = group_ids.numel()
+        if outs is None:
+            outs = [torch.empty(n_groups * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES),
+                                dtype=torch.uint8, device="cuda") for k, _ in self.aggs]
+        optr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+        arr = _columns_array(cols)
+        abi.check(lib.up_query_launch(self._h, arr, len(cols), rows, group_ids.data_ptr(), n_groups, optr,
+                                      err.data_ptr() if err is not None else None, _stream_ptr(stream)),
+                  "up_query_launch")
+        return list(outs)
+
+    def __del__(self):
+        try:
+            abi.load().up_module_release(self._h)
+        except Exception:
+            pass
+
+
+def compile_query(exprs: Sequence[Expr], aggs: Sequence[tuple[int, int]], cols: Sequence[ColType]) -> QueryModule:
+    """exprs: aggregate expressions; aggs: (kind, index into exprs)."""
+    b = build(list(exprs), cols)
+    derive_types(b)
+    return QueryModule(b, [(k, b.roots[i]) for k, i in aggs])
+
+
+def group_agg(vals: Sequence[DeviceColumn], kinds: Sequence[int], group_ids: torch.Tensor, n_groups: int,
+              err: torch.Tensor | None = None, stream=None) -> list[torch.Tensor]:
+    lib = abi.load()
+    outs = [torch.empty(n_groups * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES), dtype=torch.uint8,
+                        device="cuda") for k in kinds]
+    arr = _columns_array(vals)
+    karr = (C.c_int32 * len(kinds))(*kinds)
+    optr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+    abi.check(lib.up_group_agg(arr, karr, len(kinds), group_ids.data_ptr(), n_groups, group_ids.numel(), optr,
+                               err.data_ptr() if err is not None else None, _stream_ptr(stream)), "up_group_agg")
+    return outs
+
+
+def gen_digits(rows: int, precision: int, seed: int, signed: bool = True, nonzero: bool = False,
+               stream=None) -> torch.Tensor:
+    lib = abi.load()
+    out = torch.empty(rows * codec.compact_bytes(precision), dtype=torch.uint8, device="cuda")
+    abi.check(lib.up_util_gen_digits(out.data_ptr(), rows, precision, seed, 1 if signed else 0,
+                                     1 if nonzero else 0, _stream_ptr(stream)), "up_util_gen_digits")
+    return out
+
+
+def gen_range(rows: int, precision: int, lo: int, hi: int, step: int, seed: int, stream=None) -> torch.Tensor:
+    lib = abi.load()
+    out = torch.empty(rows * codec.compact_bytes(precision), dtype=torch.uint8, device="cuda")
+    abi.check(lib.up_util_gen_range(out.data_ptr(), rows, precision, lo, hi, step, seed, _stream_ptr(stream)),
+              "up_util_gen_range")
+    return out
+
+
+def group_ids_from_keys(keys: Sequence[torch.Tensor], key_bytes: Sequence[int], stream=None):
+    """Dense group ids in key order from fixed-width byte key columns."""
+    lib = abi.load()
+    rows = keys[0].numel() // key_bytes[0]
+    gid = torch.empty(rows, dtype=torch.int32, device="cuda")
+    total = sum(key_bytes)
+    gkeys = torch.empty(65536 * total, dtype=torch.uint8, device="cuda")
+    kp = (C.c_void_p * len(keys))(*[k.data_ptr() for k in keys])
+    kb = (C.c_int32 * len(keys))(*key_bytes)
+    n = C.c_int32()
+    abi.check(lib.up_group_ids_from_keys(kp, kb, len(keys), rows, gid.data_ptr(), C.byref(n), gkeys.data_ptr(),
+                                         _stream_ptr(stream)), "up_group_ids_from_keys")
+    return gid, n.value, gkeys[: n.value * total]
