@@ -1,4 +1,5 @@
 """GPU parity of grouped SUM/COUNT/AVG (fused and plain) against the oracle."""
+import ctypes as C
 import random
 
 import numpy as np
@@ -97,7 +98,7 @@ def test_aggregate_column_data_segments():
     ts = torch.tensor(starts, dtype=torch.int32, device="cuda")
     out = torch.empty(G * 133, dtype=torch.uint8, device="cuda")
     c = d.up_column()
-    abi.check(lib.up_aggregate_column_data(c.__class__.from_buffer_copy(c), abi.UP_AGG_SUM, ta.data_ptr(),
+    abi.check(lib.up_aggregate_column_data(C.byref(c), abi.UP_AGG_SUM, ta.data_ptr(),
                                            ts.data_ptr(), G, rows, out.data_ptr(), None,
                                            torch.cuda.current_stream().cuda_stream), "agg")
     torch.cuda.synchronize()
