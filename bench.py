@@ -38,13 +38,15 @@ METRIC = "decimal rows/s (precision sweep a*b+c and a/b, p=18..600), bit-exact"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sweep", choices=["sweep", "query"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", default="", help="comma list of p:op sweep cases (profiling a subset)")
+    ap.add_argument("--rows-scale", type=float, default=1.0, help="scale every case's rows (profiling)")
     return ap.parse_args()
 
 
@@ -71,7 +73,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                          "-lms", "50", "-i", str(self.index)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -149,7 +151,10 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     lib = abi.load()
     stream = torch.cuda.Stream()
-    cases = sweep_cases()
+    cases = sweep_cases(args.rows_scale)
+    if args.only:
+        keep = {tuple(x.split(":")) for x in args.only.split(",")}
+        cases = [c for c in cases if (str(c["p"]), c["op"]) in keep]
     hbm_peak, peak_kind = peaks()
     madd_peak = C.c_double(0)
     abi.check(lib.up_util_imad_peak(C.byref(madd_peak), stream.cuda_stream), "imad peak")
