@@ -237,6 +237,22 @@ up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64
                           const int32_t* group_ids, int32_t n_groups,
                           void* const* outs, uint32_t* err_word, void* stream);
 
+/* up_query_launch for callers that cannot allocate device memory (no
+ * counterpart in the reference; the reference allocates its aggregation
+ * buffers itself).  Same arguments and results as up_query_launch, but the
+ * per-group accumulators live in an 8 MiB file-scope device array of the
+ * library instead of stream-ordered allocations, so the call performs no
+ * cudaMalloc/cudaFree and no allocating library call.  Requests whose
+ * accumulators do not fit (n_groups x accumulator bytes + 8 bytes per group)
+ * fail with UP_ERR_INVALID_ARG.  Every GPU that loads the library holds the
+ * array until exit; all calls share it, each call clears what it uses on its
+ * stream, and calls that overlap on the GPU race.  The first call on a
+ * device looks the array up on that device: make it before any stream
+ * capture. */
+up_status up_query_launch_noalloc(up_module* m, const up_column* in, int32_t n_in, int64_t rows,
+                                  const int32_t* group_ids, int32_t n_groups,
+                                  void* const* outs, uint32_t* err_word, void* stream);
+
 /* ------------------------------------------------------------ utilities */
 /* Measured device facts used by the roofline report. */
 typedef struct up_device_info {

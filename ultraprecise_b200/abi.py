@@ -131,6 +131,7 @@ SIGNATURES = {
     "up_group_ids_from_keys": (_I32, [_P, _P, _I32, _I64, _P, _PI32, _P, _P]),
     "up_query_compile": (_I32, [_P, _I32, _P, _I32, _P, _I32, _P, C.POINTER(_P)]),
     "up_query_launch": (_I32, [_P, _P, _I32, _I64, _P, _I32, _P, _P, _P]),
+    "up_query_launch_noalloc": (_I32, [_P, _P, _I32, _I64, _P, _I32, _P, _P, _P]),
     "up_device_query": (_I32, [_I32, _P]),
 }
 
