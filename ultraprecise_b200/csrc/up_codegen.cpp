@@ -79,7 +79,7 @@ struct Emitter {
             case UP_NODE_COLUMN: {
                 const int B = compact_bytes(cols[nd.column].precision);
                 body << "    u32 " << v(k) << "[" << L << "]; u32 " << s(k) << ";\n";
-                body << "    if (TILE) ld_compact_words<" << B << ", " << L << ">(in" << nd.column << ", " << v(k)
+                body << "    if (words) ld_compact_words<" << B << ", " << L << ">(in" << nd.column << ", " << v(k)
                      << ", " << s(k) << ");\n";
                 body << "    else ld_compact_bytes<" << B << ", " << L << ">(in" << nd.column << ", " << v(k)
                      << ", " << s(k) << ");\n";
@@ -231,62 +231,134 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     Emitter em(nodes, cols, f);
     for (int k : topo) em.node(k);
 
-    const int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
-    int R = T;
+    int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
     int row_bytes = BO;
     for (int c : used) row_bytes += compact_bytes(cols[c].precision);
-    // keep a tile within ~48 KB so several CTAs share an SM
-    while (R > 32 && (long)R * row_bytes > 48 * 1024) R /= 2;
+    // Narrow rows: two pipeline stages of R rows (inputs + outputs) within
+    // ~48 KB of shared memory, R a power of two in [128, 1024].  Wide rows
+    // (fewer than 128 rows would fit): no staging, each thread reads and
+    // writes its own rows, so only registers bound the occupancy.
+    int R = 1024;
+    while (R > 128 && 2L * R * row_bytes > 48 * 1024) R /= 2;
+    const bool staged = 2L * R * row_bytes <= 48 * 1024;
+    if (staged && T > R) T = R;
 
     std::ostringstream src;
     src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << kargs_source();
-    src << "template <bool TILE>\nUP_DI u32 up_row(" << params_decl(used) << "u8* __restrict__ out) {\n";
+    src << "UP_DI u32 up_row(" << params_decl(used) << "u8* __restrict__ out, const bool words) {\n";
     src << "    u32 err = 0u;\n" << em.constants() << em.body.str();
     if (cmp_root) {
         src << "    out[0] = (u8)c" << root << ";\n";
     } else if (BO % 4 == 0) {
-        src << "    if (TILE) err |= st_compact_words<" << BO << ">(out, v" << root << ", s" << root << ");\n";
+        src << "    if (words) err |= st_compact_words<" << BO << ">(out, v" << root << ", s" << root << ");\n";
         src << "    else err |= st_compact_bytes<" << BO << ">(out, v" << root << ", s" << root << ");\n";
     } else {
         src << "    err |= st_compact_bytes<" << BO << ">(out, v" << root << ", s" << root << ");\n";
     }
     src << "    return err;\n}\n\n";
 
-    // tile kernel: contiguous columns, staged through shared memory
-    std::vector<int> off;
+    // tile kernel: contiguous columns
     int smem = 0;
-    for (int c : used) {
-        off.push_back(smem);
-        smem += ((R * compact_bytes(cols[c].precision) + 16 + 15) / 16) * 16;
+    if (staged) {
+        // double-buffered bulk-copy pipeline: stage k&1 holds tile k's inputs;
+        // the next tile's loads are issued before the current tile is
+        // computed; outputs leave through a bulk store from a double buffer
+        std::vector<int> off;
+        for (int c : used) {
+            off.push_back(smem);
+            smem += ((R * compact_bytes(cols[c].precision) + 16 + 15) / 16) * 16;
+        }
+        const int stage_in = smem;
+        const int out_bytes = ((R * BO + 16 + 15) / 16) * 16;
+        const int off_out = 2 * stage_in;
+        const int off_bar = off_out + 2 * out_bytes;
+        smem = off_bar + 16;
+        int tile_in_bytes = 0;
+        for (int c : used) tile_in_bytes += R * compact_bytes(cols[c].precision);
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_tile(const UpArgs a) {\n";
+        src << "    extern __shared__ __align__(128) u8 sm[];\n";
+        src << "    constexpr int R = " << R << ";\n";
+        src << "    u64* bar = (u64*)(sm + " << off_bar << ");\n";
+        src << "    const i64 ntiles = (a.rows + R - 1) / R;\n";
+        src << "    const i64 nfull = a.vec_ok ? a.rows / R : 0;  // tiles moved by bulk copies\n";
+        src << "    u32 err = 0u;\n";
+        src << "    if (threadIdx.x == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); mbar_init_fence(); }\n";
+        src << "    __syncthreads();\n";
+        src << "    auto issue = [&](i64 tt, int st) {\n";
+        src << "        mbar_expect_tx(&bar[st], " << tile_in_bytes << "u);\n";
+        for (size_t i = 0; i < used.size(); i++) {
+            int c = used[i];
+            int B = compact_bytes(cols[c].precision);
+            src << "        bulk_load(sm + st * " << stage_in << " + " << off[i] << ", a.col[" << c
+                << "].data + tt * (i64)(R * " << B << "), " << R * B << "u, &bar[st]);\n";
+        }
+        src << "    };\n";
+        src << "    if (threadIdx.x == 0 && (i64)blockIdx.x < nfull) issue(blockIdx.x, 0);\n";
+        src << "    int k = 0;\n";
+        src << "    bool timed_out = false;\n    int to_st = 0;\n    u32 to_par = 0u;\n";
+        src << "    for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {\n";
+        src << "        const int st = k & 1;\n";
+        src << "        const i64 row0 = t * (i64)R;\n";
+        src << "        const int nr = (a.rows - row0) < R ? (int)(a.rows - row0) : R;\n";
+        src << "        const bool bulk = t < nfull;\n";
+        src << "        const i64 tn = t + gridDim.x;\n";
+        src << "        if (threadIdx.x == 0 && tn < nfull) issue(tn, st ^ 1);\n";
+        src << "        u8* in = sm + st * " << stage_in << ";\n";
+        src << "        u8* ob = sm + " << off_out << " + st * " << out_bytes << ";\n";
+        src << "        if (bulk) {\n";
+        src << "            if (!mbar_wait(&bar[st], (u32)((k >> 1) & 1))) { timed_out = true; to_st = st; to_par = (u32)((k >> 1) & 1); }\n";
+        src << "        } else {\n";
+        for (size_t i = 0; i < used.size(); i++) {
+            int c = used[i];
+            int B = compact_bytes(cols[c].precision);
+            src << "            tile_copy_in(in + " << off[i] << ", a.col[" << c << "].data + row0 * " << B << ", nr * "
+                << B << ", a.vec_ok != 0);\n";
+        }
+        src << "            __syncthreads();\n";
+        src << "        }\n";
+        src << "        if (__syncthreads_or(timed_out)) break;\n";
+        src << "        for (int r = threadIdx.x; r < nr; r += blockDim.x)\n";
+        src << "            err |= up_row(";
+        for (size_t i = 0; i < used.size(); i++) {
+            int B = compact_bytes(cols[used[i]].precision);
+            src << "in + " << off[i] << " + r * " << B << ", ";
+        }
+        src << "ob + r * " << BO << ", true);\n";
+        src << "        if (bulk) {\n";
+        src << "            fence_async_smem();\n";
+        src << "            __syncthreads();\n";
+        src << "            if (threadIdx.x == 0) {\n";
+        src << "                bulk_store(a.out + row0 * " << BO << ", ob, " << R * BO << "u);\n";
+        src << "                bulk_commit();\n";
+        src << "                bulk_wait_read_1();\n";
+        src << "            }\n";
+        src << "        } else {\n";
+        src << "            __syncthreads();\n";
+        src << "            tile_copy_out(a.out + row0 * " << BO << ", ob, nr * " << BO << ", a.vec_ok != 0);\n";
+        src << "        }\n";
+        src << "        __syncthreads();\n";
+        src << "    }\n";
+        src << "    if (threadIdx.x == 0) {\n";
+        src << "        bulk_wait_all();\n";
+        src << "        if (timed_out) {\n";
+        src << "            err |= ERR_TIMEOUT;\n";
+        src << "            mbar_wait(&bar[to_st], to_par);  // bounded: let copies in flight land before exit\n";
+        src << "        }\n";
+        src << "    }\n";
+    } else {
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_tile(const UpArgs a) {\n";
+        src << "    u32 err = 0u;\n";
+        src << "    const i64 stride = (i64)gridDim.x * blockDim.x;\n";
+        src << "    for (i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x; row < a.rows; row += stride) {\n";
+        src << "        const bool words = a.vec_ok != 0 && row + 1 < a.rows;  // word reads stay inside the column\n";
+        src << "        err |= up_row(";
+        for (int c : used) {
+            int B = compact_bytes(cols[c].precision);
+            src << "a.col[" << c << "].data + row * " << B << ", ";
+        }
+        src << "a.out + row * " << BO << ", words);\n";
+        src << "    }\n";
     }
-    const int off_out = smem;
-    smem += ((R * BO + 16 + 15) / 16) * 16;
-
-    src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_tile(const UpArgs a) {\n";
-    src << "    extern __shared__ __align__(16) u8 sm[];\n";
-    src << "    constexpr int R = " << R << ";\n";
-    src << "    const i64 ntiles = (a.rows + R - 1) / R;\n    u32 err = 0u;\n";
-    src << "    for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x) {\n";
-    src << "        const i64 row0 = t * (i64)R;\n";
-    src << "        const int nr = (a.rows - row0) < R ? (int)(a.rows - row0) : R;\n";
-    for (size_t i = 0; i < used.size(); i++) {
-        int c = used[i];
-        int B = compact_bytes(cols[c].precision);
-        src << "        tile_copy_in(sm + " << off[i] << ", a.col[" << c << "].data + row0 * " << B << ", nr * " << B
-            << ", a.vec_ok != 0);\n";
-    }
-    src << "        __syncthreads();\n";
-    src << "        for (int r = threadIdx.x; r < nr; r += blockDim.x)\n";
-    src << "            err |= up_row<true>(";
-    for (size_t i = 0; i < used.size(); i++) {
-        int B = compact_bytes(cols[used[i]].precision);
-        src << "sm + " << off[i] << " + r * " << B << ", ";
-    }
-    src << "sm + " << off_out << " + r * " << BO << ");\n";
-    src << "        __syncthreads();\n";
-    src << "        tile_copy_out(a.out + row0 * " << BO << ", sm + " << off_out << ", nr * " << BO
-        << ", a.vec_ok != 0);\n";
-    src << "        __syncthreads();\n    }\n";
     src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
     src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
 
@@ -312,9 +384,9 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     } else {
         src << "        if (isnull) { err |= ERR_DOMAIN; for (int i = 0; i < " << BO << "; i++) o[i] = 0; continue; }\n";
     }
-    src << "        err |= up_row<false>(";
+    src << "        err |= up_row(";
     for (int c : used) src << "in" << c << ", ";
-    src << "o);\n    }\n";
+    src << "o, false);\n    }\n";
     src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
     src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n";
 
@@ -325,7 +397,7 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     out.out_bytes = OB;
     out.out_is_compare = cmp_root;
     out.block_threads = T;
-    out.tile_rows = R;
+    out.tile_rows = staged ? R : T;
     out.smem_bytes = smem;
     out.in_bytes.assign(n_cols, 0);
     for (int c = 0; c < n_cols; c++) out.in_bytes[c] = compact_bytes(cols[c].precision) + (cols[c].nullable ? 1 : 0);
@@ -398,7 +470,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     const int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
     std::ostringstream src;
     src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << kargs_source();
-    src << "template <bool TILE>\nUP_DI u32 up_qrow(" << params_decl(used) << "u32* __restrict__ acc) {\n";
+    src << "UP_DI u32 up_qrow(" << params_decl(used) << "u32* __restrict__ acc, const bool words) {\n";
     src << "    u32 err = 0u;\n" << em.constants() << em.body.str();
     for (int a = 0; a < n_aggs; a++) {
         if (aggs[a].kind == UP_AGG_COUNT) continue;
@@ -423,9 +495,9 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
             src << "        else { if (in" << c << "[0] == 0) isnull = true; in" << c << " += 1; }\n";
     }
     src << "        if (isnull) continue;\n";
-    src << "        err |= up_qrow<false>(";
+    src << "        err |= up_qrow(";
     for (int c : used) src << "in" << c << ", ";
-    src << "a.acc + (i64)g * " << std::max(accw, 1) << ");\n    }\n";
+    src << "a.acc + (i64)g * " << std::max(accw, 1) << ", false);\n    }\n";
     src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
     src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
 

@@ -219,24 +219,49 @@ UP_DI void shr_bits(u32 (&r)[N], const u32 (&a)[N], u32 s) {
 }
 
 // ------------------------------------------------------------ division
+// 2/1 division by a normalised 32-bit divisor with a precomputed reciprocal:
+// Moller & Granlund, "Improved division by invariant integers" (IEEE Trans.
+// Computers, 2011), Algorithm 4.  d has its top bit set, v = floor((2^64-1)/d)
+// - 2^32, and u1 < d; returns q = floor((u1*2^32 + u0)/d), r the remainder.
+UP_DI u32 reciprocal_u32(u32 d) { return (u32)(0xffffffffffffffffull / d); }
+
+UP_DI u32 div2by1(u32 u1, u32 u0, u32 d, u32 v, u32& r) {
+    u64 q = (u64)v * u1;
+    q += ((u64)u1 << 32) | u0;
+    u32 q1 = (u32)(q >> 32) + 1u;
+    const u32 q0 = (u32)q;
+    u32 rr = u0 - q1 * d;
+    if (rr > q0) {
+        q1 -= 1u;
+        rr += d;
+    }
+    if (rr >= d) {
+        q1 += 1u;
+        rr -= d;
+    }
+    r = rr;
+    return q1;
+}
+
 // Knuth, TAOCP vol. 2, 4.3.1, Algorithm D in base 2^32 with static array
 // sizes: the divisor is normalised to exactly NB limbs (top bit set) by a
-// dynamic left shift applied to both operands, so the quotient loop runs a
-// fixed NX+1 steps and every array stays in registers for small sizes.
+// dynamic left shift applied to both operands; quotient steps above the
+// dividend's actual length are skipped (their digits are zero).  Quotient
+// digit estimates use the 2/1 reciprocal division above.
 // q = floor(x / b), rem = x mod b.  Requires b != 0.
 template <int NX, int NB>
 UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&b)[NB]) {
     if constexpr (NB == 1) {
-        const u32 d = b[0];
-        u64 r = 0;
+        const u32 sh = (u32)__clz(b[0]);
+        const u32 d = b[0] << sh;
+        const u32 v = reciprocal_u32(d);
+        u32 r = sh ? (x[NX - 1] >> (32u - sh)) : 0u;
 #pragma unroll
         for (int i = NX - 1; i >= 0; i--) {
-            u64 cur = (r << 32) | x[i];
-            u64 qq = cur / d;
-            q[i] = (u32)qq;
-            r = cur - qq * d;
+            const u32 lo = sh ? __funnelshift_l(i > 0 ? x[i > 0 ? i - 1 : 0] : 0u, x[i], sh) : x[i];
+            q[i] = div2by1(r, lo, d, v, r);
         }
-        rem[0] = (u32)r;
+        rem[0] = r >> sh;
     } else {
     constexpr int NU = NX + NB + 1;
     const u32 bl = bitlen(b);
@@ -251,15 +276,29 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
     }
     const u32 vtop = bn[NB - 1];
     const u32 vnext = bn[NB - 2];
-#pragma unroll(((NX + 1) * NB <= 96) ? NX + 1 : 1)
+    const u32 vinv = reciprocal_u32(vtop);
+    // quotient digits above nx - nb + 1 are zero (x < 2^(32 nx), b >= 2^(32 (nb-1)))
+    const int jmax = (int)((bitlen(x) + 31u) >> 5) - (int)((bl + 31u) >> 5) + 1;
+    constexpr bool kUnroll = (NX + 1) * NB <= 96;
+#pragma unroll(kUnroll ? NX + 1 : 1)
     for (int j = NX; j >= 0; j--) {
-        const u64 num = ((u64)un[j + NB] << 32) | un[j + NB - 1];
-        u64 qhat = num / vtop;
-        u64 rhat = num - qhat * vtop;
-        while ((qhat >> 32) != 0u || qhat * vnext > ((rhat << 32) | un[j + NB - 2])) {
+        if (j > jmax) {
+            if (j < NX) q[j < NX ? j : 0] = 0u;
+            continue;
+        }
+        const u32 u1 = un[j + NB], u0 = un[j + NB - 1];
+        u64 qhat, rhat;
+        if (u1 >= vtop) {
+            qhat = 0xffffffffull;
+            rhat = (u64)u0 + vtop;
+        } else {
+            u32 r32;
+            qhat = div2by1(u1, u0, vtop, vinv, r32);
+            rhat = r32;
+        }
+        while ((rhat >> 32) == 0u && qhat * vnext > ((rhat << 32) | un[j + NB - 2])) {
             qhat--;
             rhat += vtop;
-            if (rhat >> 32) break;
         }
         // multiply and subtract qhat * bn from un[j .. j+NB]
         u64 carry = 0;
@@ -285,7 +324,7 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
             }
             un[j + NB] += (u32)c;
         }
-        if (j < NX) q[j] = (u32)qhat;
+        if (j < NX) q[j < NX ? j : 0] = (u32)qhat;
     }
     u32 rl[NB];
 #pragma unroll
@@ -592,6 +631,66 @@ UP_DI void agg_image(u8* img, u32 flag, u32 sign, u32 frac, const u32 (&m)[N]) {
         img[8 + 4 * i] = (u8)(w >> 24);
     }
 }
+
+// ------------------------------------------------- bulk-copy pipeline
+// 1-D bulk copies (cp.async.bulk, the TMA engine without a tensor map) between
+// global and shared memory, completed through an mbarrier.  Sizes are
+// multiples of 16 bytes and both addresses 16-byte aligned (the callers only
+// use them for full tiles of 16-byte-aligned columns).  No multicast.
+enum : u32 { ERR_TIMEOUT = 8u };
+
+UP_DI u32 smem_addr(const void* p) {
+    u32 r;
+    asm volatile("{ .reg .u64 t; cvta.to.shared.u64 t, %1; cvt.u32.u64 %0, t; }" : "=r"(r) : "l"(p));
+    return r;
+}
+
+UP_DI void mbar_init(u64* bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+UP_DI void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+UP_DI void mbar_expect_tx(u64* bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+UP_DI void bulk_load(void* dst_smem, const void* src_gmem, u32 bytes, u64* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst_smem)),
+        "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Wait for the mbarrier phase with the given parity; gives up after a bounded
+// number of polls and returns false (the caller records ERR_TIMEOUT).
+UP_DI bool mbar_wait(u64* bar, u32 parity) {
+    const u32 a = smem_addr(bar);
+    for (u32 it = 0; it < (1u << 24); it++) {
+        u32 done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+UP_DI void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+UP_DI void bulk_store(void* dst_gmem, const void* src_smem, u32 bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem),
+                 "r"(smem_addr(src_smem)), "r"(bytes)
+                 : "memory");
+}
+
+UP_DI void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+UP_DI void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+UP_DI void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 }  // namespace up
 
