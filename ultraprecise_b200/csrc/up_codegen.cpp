@@ -235,14 +235,17 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     int row_bytes = BO;
     for (int c : used) row_bytes += compact_bytes(cols[c].precision);
     // Narrow rows: two pipeline stages of R rows (inputs + outputs) within
-    // ~48 KB of shared memory, R a power of two in [128, 1024].  Wide rows
-    // (fewer than 128 rows would fit): no staging, each thread reads and
-    // writes its own rows, so only registers bound the occupancy.
+    // ~48 KB of shared memory, R a power of two in [128, 1024], moved by bulk
+    // copies.  Wide rows: one synchronously staged tile of R rows (R >= 32)
+    // and a CTA of min(256, R) threads, so no thread idles at the barriers.
     int R = 1024;
     while (R > 128 && 2L * R * row_bytes > 48 * 1024) R /= 2;
     const bool staged = 2L * R * row_bytes <= 48 * 1024;
-    if (staged && T > R) T = R;
-
+    if (!staged) {
+        R = 1024;
+        while (R > 32 && (long)R * row_bytes > 48 * 1024) R /= 2;
+    }
+    if (T > R) T = R;
     std::ostringstream src;
     src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << kargs_source();
     src << "UP_DI u32 up_row(" << params_decl(used) << "u8* __restrict__ out, const bool words) {\n";
@@ -346,18 +349,39 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
         src << "        }\n";
         src << "    }\n";
     } else {
-        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_tile(const UpArgs a) {\n";
-        src << "    u32 err = 0u;\n";
-        src << "    const i64 stride = (i64)gridDim.x * blockDim.x;\n";
-        src << "    for (i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x; row < a.rows; row += stride) {\n";
-        src << "        const bool words = a.vec_ok != 0 && row + 1 < a.rows;  // word reads stay inside the column\n";
-        src << "        err |= up_row(";
+        // one synchronously staged tile per iteration (wide rows)
+        std::vector<int> off;
         for (int c : used) {
-            int B = compact_bytes(cols[c].precision);
-            src << "a.col[" << c << "].data + row * " << B << ", ";
+            off.push_back(smem);
+            smem += ((R * compact_bytes(cols[c].precision) + 16 + 15) / 16) * 16;
         }
-        src << "a.out + row * " << BO << ", words);\n";
-        src << "    }\n";
+        const int off_out = smem;
+        smem += ((R * BO + 16 + 15) / 16) * 16;
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_tile(const UpArgs a) {\n";
+        src << "    extern __shared__ __align__(16) u8 sm[];\n";
+        src << "    constexpr int R = " << R << ";\n";
+        src << "    const i64 ntiles = (a.rows + R - 1) / R;\n    u32 err = 0u;\n";
+        src << "    for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x) {\n";
+        src << "        const i64 row0 = t * (i64)R;\n";
+        src << "        const int nr = (a.rows - row0) < R ? (int)(a.rows - row0) : R;\n";
+        for (size_t i = 0; i < used.size(); i++) {
+            int c = used[i];
+            int B = compact_bytes(cols[c].precision);
+            src << "        tile_copy_in(sm + " << off[i] << ", a.col[" << c << "].data + row0 * " << B << ", nr * "
+                << B << ", a.vec_ok != 0);\n";
+        }
+        src << "        __syncthreads();\n";
+        src << "        for (int r = threadIdx.x; r < nr; r += blockDim.x)\n";
+        src << "            err |= up_row(";
+        for (size_t i = 0; i < used.size(); i++) {
+            int B = compact_bytes(cols[used[i]].precision);
+            src << "sm + " << off[i] << " + r * " << B << ", ";
+        }
+        src << "sm + " << off_out << " + r * " << BO << ", true);\n";
+        src << "        __syncthreads();\n";
+        src << "        tile_copy_out(a.out + row0 * " << BO << ", sm + " << off_out << ", nr * " << BO
+            << ", a.vec_ok != 0);\n";
+        src << "        __syncthreads();\n    }\n";
     }
     src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
     src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
@@ -397,7 +421,7 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     out.out_bytes = OB;
     out.out_is_compare = cmp_root;
     out.block_threads = T;
-    out.tile_rows = staged ? R : T;
+    out.tile_rows = R;
     out.smem_bytes = smem;
     out.in_bytes.assign(n_cols, 0);
     for (int c = 0; c < n_cols; c++) out.in_bytes[c] = compact_bytes(cols[c].precision) + (cols[c].nullable ? 1 : 0);
