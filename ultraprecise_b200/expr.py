@@ -222,3 +222,18 @@ def derive_types(b: Built, root: int | None = None) -> Built:
 
 def node_type(b: Built, k: int) -> tuple[int, int]:
     return b.nodes[k].precision, b.nodes[k].scale
+
+
+def align_optimize(b: Built, root: int | None = None, cap: int = 4096) -> Built:
+    """The reference's AlignOptimize rewrite (AriesEngineShell.cpp:244-685)
+    on one root; returns a new Built whose single root is the rewritten tree."""
+    lib = abi.load()
+    r = b.roots[0] if root is None else root
+    out = (abi.UpExprNode * cap)()
+    n = C.c_int32()
+    nr = C.c_int32()
+    abi.check(lib.up_expr_align_optimize(b.nodes, b.n_nodes, r, b.col_types, b.n_cols, out, cap, C.byref(n),
+                                         C.byref(nr)), "up_expr_align_optimize")
+    arr = (abi.UpExprNode * max(1, n.value))()
+    C.memmove(arr, out, C.sizeof(abi.UpExprNode) * n.value)
+    return Built(arr, n.value, [nr.value], b.col_types, b.n_cols, [])
