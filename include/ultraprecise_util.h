@@ -45,6 +45,11 @@ up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32
                                const up_col_type* cols, int32_t n_cols, int32_t query,
                                const up_query_agg* aggs, int32_t n_aggs);
 
+/* The same for a batch module (ultraprecise_batch.h): generate and compile
+ * every task into one CUBIN without loading it. */
+struct up_batch_task;
+up_status up_util_compile_batch_only(const struct up_batch_task* tasks, int32_t n_tasks);
+
 #ifdef __cplusplus
 }
 #endif

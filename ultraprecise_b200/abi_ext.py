@@ -13,4 +13,12 @@ SIGNATURES = {
     "up_util_flush_l2": (_I32, [_P, _I64, _P]),
     "up_util_imad_peak": (_I32, [C.POINTER(C.c_double), _P]),
     "up_util_compile_only": (_I32, [_P, _I32, _I32, _P, _I32, _I32, _P, _I32]),
+    # ultraprecise_batch.h
+    "up_batch_create": (_I32, [_P, _I32, _P, C.POINTER(_P)]),
+    "up_batch_bind": (_I32, [_P, _I32, _P, _I32, _I64, _P, _I32, _P]),
+    "up_batch_launch": (_I32, [_P, _P, _P]),
+    "up_batch_shape": (_I32, [_P, _I32, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32), C.POINTER(C.c_double)]),
+    "up_batch_task_type": (_I32, [_P, _I32, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32)]),
+    "up_batch_release": (None, [_P]),
+    "up_util_compile_batch_only": (_I32, [_P, _I32]),
 }

@@ -1,0 +1,523 @@
+// up_batch.cpp — batched persistent-kernel mode (include/ultraprecise_batch.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/ultraprecise_batch.h"
+#include "../../include/ultraprecise_util.h"
+#include "up_internal.h"
+
+using namespace upi;
+
+namespace {
+
+struct HKCol {
+    const void* data;
+    const void* const* blocks;
+    const int64_t* prefix;
+    const int32_t* indices;
+    int32_t n_blocks;
+    int32_t value_bytes;
+};
+// host mirror of the generated BTask / BArgs (generate_batch_module)
+struct HBTask {
+    HKCol col[8];
+    int64_t rows;
+    uint8_t* out;
+    const int32_t* gid;
+    uint32_t* acc;
+    uint64_t* cnt;
+    int32_t n_groups;
+    int32_t words;
+};
+static_assert(sizeof(HBTask) == 368, "BTask layout");
+struct HBArgs {
+    void* tasks;
+    const int32_t* item_task;
+    const int64_t* item_tile;
+    int64_t n_items;
+    unsigned long long* head;
+    uint32_t* err;
+    int32_t tile_rows;
+    int32_t pad;
+};
+static_assert(sizeof(HBArgs) == 56, "BArgs layout");
+
+const int kThreads[3] = {64, 128, 256};
+
+up_status cuda_err(cudaError_t e, const std::string& what) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? UP_ERR_NO_MEMORY : UP_ERR_CUDA, what + ": " + cudaGetErrorString(e));
+}
+
+#define UPB_CUDA(call)                                     \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_err(e_, #call); \
+    } while (0)
+
+struct Shape {
+    int threads_idx = 2;  // index into kThreads
+    int ctas_per_sm = 4;
+    int tile_rows = 1024;
+    double tuned_ms = 0.0;
+};
+
+std::string autotune_path() {
+    const char* p = getenv("UP_AUTOTUNE_CACHE");
+    if (p && *p) return p;
+    const char* d = getenv("UP_JIT_CACHE_DIR");
+    if (d && *d) return std::string(d) + "/autotune.txt";
+    const char* home = getenv("HOME");
+    return std::string(home && *home ? home : "/tmp") + "/.cache/ultraprecise_b200/autotune.txt";
+}
+
+uint64_t fnv(const std::string& s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+}  // namespace
+
+struct up_batch {
+    GeneratedBatch gen;
+    std::shared_ptr<JitKernelSet> ks;
+    up_batch_opts opts{};
+    std::vector<HBTask> host_tasks;
+    std::vector<bool> bound;
+    std::vector<double> cost;  // per-row cost estimate per task
+    void* d_tasks = nullptr;
+    int64_t n_items[3] = {0, 0, 0};
+    int32_t* item_task[3] = {nullptr, nullptr, nullptr};
+    int64_t* item_tile[3] = {nullptr, nullptr, nullptr};
+    int items_tile_rows[3] = {0, 0, 0};
+    unsigned long long* heads = nullptr;
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int max_groups = 0;
+    bool prepared = false;
+    Shape shape[3];
+    bool tuned = false;
+    cudaGraphExec_t gexec = nullptr;
+    uint32_t* graph_err = nullptr;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    std::string key;
+    void drop_graph() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+    }
+    void drop_device() {
+        drop_graph();
+        if (d_tasks) cudaFree(d_tasks);
+        if (heads) cudaFree(heads);
+        if (scratch) cudaFree(scratch);
+        d_tasks = nullptr;
+        heads = nullptr;
+        scratch = nullptr;
+        for (int band = 0; band < 3; band++) {
+            if (item_task[band]) cudaFree(item_task[band]);
+            item_task[band] = nullptr;
+            item_tile[band] = nullptr;
+            items_tile_rows[band] = 0;
+        }
+        prepared = false;
+    }
+    ~up_batch() {
+        drop_device();
+        for (int i = 0; i < 2; i++) {
+            if (side[i]) cudaStreamDestroy(side[i]);
+            if (join[i]) cudaEventDestroy(join[i]);
+        }
+        if (fork) cudaEventDestroy(fork);
+    }
+};
+
+namespace {
+
+// (Re)build one band's work list for a given rows-per-item: every item of a
+// costlier task precedes the items of cheaper ones (longest-processing-time
+// order), tiles of a task in order.
+up_status build_items(up_batch* b, int band, int tile_rows) {
+    if (b->items_tile_rows[band] == tile_rows && b->item_task[band]) return UP_OK;
+    std::vector<int> order;
+    for (size_t k = 0; k < b->gen.tasks.size(); k++)
+        if (b->gen.tasks[k].band == band && b->host_tasks[k].rows > 0) order.push_back((int)k);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->cost[x] > b->cost[y]; });
+    std::vector<int32_t> it;
+    std::vector<int64_t> tl;
+    for (int k : order) {
+        const int64_t nt = (b->host_tasks[k].rows + tile_rows - 1) / tile_rows;
+        for (int64_t t = 0; t < nt; t++) {
+            it.push_back(k);
+            tl.push_back(t);
+        }
+    }
+    if (b->item_task[band]) {
+        cudaFree(b->item_task[band]);
+        b->item_task[band] = nullptr;
+        b->item_tile[band] = nullptr;
+    }
+    b->n_items[band] = (int64_t)it.size();
+    b->items_tile_rows[band] = tile_rows;
+    if (it.empty()) return UP_OK;
+    void* mem = nullptr;
+    const size_t bytes_t = ((it.size() * 4) + 15) & ~size_t(15), bytes_l = tl.size() * 8;
+    UPB_CUDA(cudaMalloc(&mem, bytes_t + bytes_l));
+    b->item_task[band] = (int32_t*)mem;
+    b->item_tile[band] = (int64_t*)((uint8_t*)mem + bytes_t);
+    UPB_CUDA(cudaMemcpy(b->item_task[band], it.data(), it.size() * 4, cudaMemcpyHostToDevice));
+    UPB_CUDA(cudaMemcpy(b->item_tile[band], tl.data(), bytes_l, cudaMemcpyHostToDevice));
+    return UP_OK;
+}
+
+HBArgs band_args(up_batch* b, int band, uint32_t* err) {
+    HBArgs a;
+    memset(&a, 0, sizeof a);
+    a.tasks = b->d_tasks;
+    a.item_task = b->item_task[band];
+    a.item_tile = b->item_tile[band];
+    a.n_items = b->n_items[band];
+    a.head = b->heads + band;
+    a.err = err;
+    a.tile_rows = b->items_tile_rows[band];
+    return a;
+}
+
+up_status launch_band(up_batch* b, int band, uint32_t* err, cudaStream_t s) {
+    if (b->n_items[band] == 0) return UP_OK;
+    const Shape& sh = b->shape[band];
+    const std::string name = "up_batch_b" + std::to_string(band) + "_t" + std::to_string(kThreads[sh.threads_idx]);
+    void* k = jit_kernel(*b->ks, name);
+    if (!k) return fail(UP_ERR_CUDA, "missing kernel " + name);
+    HBArgs a = band_args(b, band, err);
+    void* args[1] = {&a};
+    const int sms = std::max(1, sm_count_current());
+    int64_t grid = std::min<int64_t>((int64_t)sms * sh.ctas_per_sm, b->n_items[band]);
+    UPB_CUDA(cudaLaunchKernel((const void*)k, dim3((unsigned)std::max<int64_t>(grid, 1)),
+                              dim3(kThreads[sh.threads_idx]), args, 0, s));
+    return UP_OK;
+}
+
+up_status launch_fin(up_batch* b, uint32_t* err, cudaStream_t s) {
+    if (b->gen.agg_tasks.empty() || b->max_groups == 0) return UP_OK;
+    void* k = jit_kernel(*b->ks, "up_batch_fin");
+    HBArgs a = band_args(b, 0, err);
+    void* args[1] = {&a};
+    dim3 grid((unsigned)((b->max_groups + 255) / 256), (unsigned)b->gen.agg_tasks.size());
+    UPB_CUDA(cudaLaunchKernel((const void*)k, grid, dim3(256), args, 0, s));
+    return UP_OK;
+}
+
+up_status clear_state(up_batch* b, cudaStream_t s) {
+    UPB_CUDA(cudaMemsetAsync(b->heads, 0, 3 * sizeof(unsigned long long), s));
+    if (b->scratch_bytes) UPB_CUDA(cudaMemsetAsync(b->scratch, 0, b->scratch_bytes, s));
+    return UP_OK;
+}
+
+// one full step: clear, the three bands forked across streams, finalise
+up_status run_step(up_batch* b, uint32_t* err, cudaStream_t s) {
+    up_status st = clear_state(b, s);
+    if (st != UP_OK) return st;
+    UPB_CUDA(cudaEventRecord(b->fork, s));
+    for (int i = 0; i < 2; i++) UPB_CUDA(cudaStreamWaitEvent(b->side[i], b->fork, 0));
+    if ((st = launch_band(b, 0, err, s)) != UP_OK) return st;
+    if ((st = launch_band(b, 1, err, b->side[0])) != UP_OK) return st;
+    if ((st = launch_band(b, 2, err, b->side[1])) != UP_OK) return st;
+    for (int i = 0; i < 2; i++) {
+        UPB_CUDA(cudaEventRecord(b->join[i], b->side[i]));
+        UPB_CUDA(cudaStreamWaitEvent(s, b->join[i], 0));
+    }
+    return launch_fin(b, err, s);
+}
+
+up_status prepare(up_batch* b) {
+    if (b->prepared) return UP_OK;
+    const size_t nt = b->host_tasks.size();
+    size_t off = 0;
+    std::vector<size_t> acc_off(nt, 0), cnt_off(nt, 0);
+    b->max_groups = 0;
+    for (size_t k = 0; k < nt; k++) {
+        const auto& gt = b->gen.tasks[k];
+        if (gt.agg < 0) continue;
+        const int G = b->host_tasks[k].n_groups;
+        b->max_groups = std::max(b->max_groups, G);
+        acc_off[k] = off;
+        off += (((size_t)G * std::max(gt.nacc, 1) * 4u) + 15u) & ~size_t(15);
+        cnt_off[k] = off;
+        off = (off + (size_t)G * 8u + 15u) & ~size_t(15);
+    }
+    b->scratch_bytes = off;
+    if (off) UPB_CUDA(cudaMalloc(&b->scratch, off));
+    for (size_t k = 0; k < nt; k++) {
+        if (b->gen.tasks[k].agg < 0) continue;
+        b->host_tasks[k].acc = (uint32_t*)((uint8_t*)b->scratch + acc_off[k]);
+        b->host_tasks[k].cnt = (uint64_t*)((uint8_t*)b->scratch + cnt_off[k]);
+    }
+    UPB_CUDA(cudaMalloc(&b->d_tasks, nt * sizeof(HBTask)));
+    UPB_CUDA(cudaMemcpy(b->d_tasks, b->host_tasks.data(), nt * sizeof(HBTask), cudaMemcpyHostToDevice));
+    UPB_CUDA(cudaMalloc((void**)&b->heads, 3 * sizeof(unsigned long long)));
+    for (int i = 0; i < 2; i++) {
+        if (!b->side[i]) UPB_CUDA(cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking));
+        if (!b->join[i]) UPB_CUDA(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming));
+    }
+    if (!b->fork) UPB_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (int band = 0; band < 3; band++) {
+        up_status st = build_items(b, band, b->shape[band].tile_rows);
+        if (st != UP_OK) return st;
+    }
+    b->prepared = true;
+    return UP_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+bool load_tuned(up_batch* b) {
+    std::ifstream f(autotune_path());
+    if (!f) return false;
+    std::string line;
+    int found = 0;
+    Shape tmp[3];
+    while (std::getline(f, line)) {
+        std::istringstream ss(line);
+        std::string key;
+        int band, ti, ctas, tr;
+        double ms;
+        if (!(ss >> key >> band >> ti >> ctas >> tr >> ms)) continue;
+        if (key != b->key || band < 0 || band > 2 || ti < 0 || ti > 2 || ctas < 1 || tr < 1) continue;
+        tmp[band] = Shape{ti, ctas, tr, ms};
+        found |= 1 << band;
+    }
+    if (found != 7) return false;
+    for (int i = 0; i < 3; i++) b->shape[i] = tmp[i];
+    return true;
+}
+
+void save_tuned(up_batch* b) {
+    const std::string p = autotune_path();
+    const std::string dir = p.substr(0, p.rfind('/'));
+    for (size_t i = 1; i <= dir.size(); i++)
+        if (i == dir.size() || dir[i] == '/') mkdir_if_missing(dir.substr(0, i));
+    std::ofstream f(p, std::ios::app);
+    for (int band = 0; band < 3; band++) {
+        const Shape& s = b->shape[band];
+        f << b->key << " " << band << " " << s.threads_idx << " " << s.ctas_per_sm << " " << s.tile_rows << " "
+          << s.tuned_ms << "\n";
+    }
+}
+
+// Sweep block size x CTAs per SM x rows per work item for each band, timing
+// that band's kernel alone with CUDA events; keep the fastest shape.
+up_status autotune(up_batch* b, cudaStream_t s) {
+    if (load_tuned(b)) {
+        for (int band = 0; band < 3; band++) {
+            up_status st = build_items(b, band, b->shape[band].tile_rows);
+            if (st != UP_OK) return st;
+        }
+        b->tuned = true;
+        return UP_OK;
+    }
+    cudaEvent_t e0, e1;
+    UPB_CUDA(cudaEventCreate(&e0));
+    UPB_CUDA(cudaEventCreate(&e1));
+    static const int kCtas[] = {1, 2, 4, 8};
+    static const int kTiles[] = {256, 1024, 4096};
+    up_status st = UP_OK;
+    for (int band = 0; band < 3 && st == UP_OK; band++) {
+        bool any = false;
+        for (size_t k = 0; k < b->gen.tasks.size(); k++)
+            if (b->gen.tasks[k].band == band && b->host_tasks[k].rows > 0) any = true;
+        if (!any) continue;
+        Shape best = b->shape[band];
+        best.tuned_ms = 1e30;
+        for (int tr : kTiles) {
+            if ((st = build_items(b, band, tr)) != UP_OK) break;
+            for (int ti = 0; ti < 3 && st == UP_OK; ti++)
+                for (int c : kCtas) {
+                    b->shape[band] = Shape{ti, c, tr, 0.0};
+                    double best_rep = 1e30;
+                    for (int rep = 0; rep < 2; rep++) {
+                        if ((st = clear_state(b, s)) != UP_OK) break;
+                        cudaEventRecord(e0, s);
+                        if ((st = launch_band(b, band, nullptr, s)) != UP_OK) break;
+                        cudaEventRecord(e1, s);
+                        cudaEventSynchronize(e1);
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        best_rep = std::min(best_rep, (double)ms);
+                    }
+                    if (st != UP_OK) break;
+                    if (best_rep < best.tuned_ms) best = Shape{ti, c, tr, best_rep};
+                }
+        }
+        b->shape[band] = best;
+        if (st == UP_OK) st = build_items(b, band, best.tile_rows);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != UP_OK) return st;
+    b->tuned = true;
+    save_tuned(b);
+    return UP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+up_status up_batch_create(const up_batch_task* tasks, int32_t n_tasks, const up_batch_opts* opts, up_batch** out) {
+    if (!tasks || !out || n_tasks <= 0) return fail(UP_ERR_INVALID_ARG, "no tasks");
+    *out = nullptr;
+    std::vector<BatchTaskDesc> desc(n_tasks);
+    for (int k = 0; k < n_tasks; k++)
+        desc[k] = BatchTaskDesc{tasks[k].nodes, tasks[k].n_nodes, tasks[k].root, tasks[k].cols, tasks[k].n_cols,
+                                tasks[k].agg_kind};
+    auto* b = new up_batch();
+    up_status st = generate_batch_module(desc.data(), n_tasks, b->gen);
+    if (st == UP_OK) {
+        std::vector<char> cubin;
+        st = jit_compile_linked(b->gen.units, cubin);
+        if (st == UP_OK) st = jit_load(cubin, b->gen.kernels, b->ks);
+    }
+    if (st != UP_OK) {
+        delete b;
+        return st;
+    }
+    if (opts) b->opts = *opts;
+    else b->opts.use_graph = 1;
+    b->host_tasks.assign(n_tasks, HBTask());
+    memset(b->host_tasks.data(), 0, sizeof(HBTask) * n_tasks);
+    b->bound.assign(n_tasks, false);
+    b->cost.assign(n_tasks, 1.0);
+    for (int k = 0; k < n_tasks; k++) {
+        // per-row cost estimate: limb products of every node
+        std::vector<NodeFacts> f;
+        std::vector<int> topo;
+        analyze_nodes(tasks[k].nodes, tasks[k].n_nodes, tasks[k].cols, tasks[k].n_cols, f, topo, {tasks[k].root});
+        double c = 0;
+        for (int n : topo) c += (double)f[n].limbs * f[n].limbs;
+        b->cost[k] = c;
+    }
+    for (int band = 0; band < 3; band++) {
+        Shape& s = b->shape[band];
+        if (b->opts.block_threads == 64) s.threads_idx = 0;
+        else if (b->opts.block_threads == 128) s.threads_idx = 1;
+        else if (b->opts.block_threads == 256) s.threads_idx = 2;
+        else s.threads_idx = band == 2 ? 0 : 2;
+        s.ctas_per_sm = b->opts.ctas_per_sm > 0 ? b->opts.ctas_per_sm : (band == 2 ? 8 : 4);
+        s.tile_rows = b->opts.tile_rows > 0 ? b->opts.tile_rows : (band == 2 ? 256 : 1024);
+    }
+    char key[40];
+    snprintf(key, sizeof key, "%016llx", (unsigned long long)fnv(b->gen.source));
+    b->key = key;
+    *out = b;
+    return UP_OK;
+}
+
+up_status up_batch_bind(up_batch* b, int32_t task, const up_column* in, int32_t n_in, int64_t rows,
+                        const int32_t* group_ids, int32_t n_groups, void* out) {
+    if (!b || task < 0 || task >= (int)b->gen.tasks.size()) return fail(UP_ERR_INVALID_ARG, "bad task");
+    const auto& gt = b->gen.tasks[task];
+    if (n_in < (int)gt.in_bytes.size() || (n_in > 0 && !in)) return fail(UP_ERR_INVALID_ARG, "too few columns");
+    if (rows < 0 || !out) return fail(UP_ERR_INVALID_ARG, "bad rows or output");
+    if (gt.agg >= 0 && (n_groups < 0 || (rows > 0 && !group_ids))) return fail(UP_ERR_INVALID_ARG, "bad groups");
+    HBTask& h = b->host_tasks[task];
+    memset(&h.col, 0, sizeof h.col);
+    bool words = true;
+    for (int c = 0; c < (int)gt.in_bytes.size(); c++) {
+        if (in[c].value_bytes != gt.in_bytes[c] || !in[c].data || in[c].n_blocks > 0 || in[c].indices ||
+            in[c].nullable)
+            return fail(UP_ERR_INVALID_ARG, "batch tasks take contiguous non-null columns of the compiled width");
+        h.col[c].data = in[c].data;
+        h.col[c].value_bytes = in[c].value_bytes;
+        if (((uintptr_t)in[c].data & 3u) != 0) words = false;
+    }
+    h.rows = rows;
+    h.out = (uint8_t*)out;
+    h.gid = group_ids;
+    h.n_groups = gt.agg >= 0 ? n_groups : 0;
+    h.words = words ? 1 : 0;
+    b->bound[task] = true;
+    b->drop_device();  // device copies and the graph are rebuilt on the next launch
+    return UP_OK;
+}
+
+up_status up_batch_launch(up_batch* b, uint32_t* err_word, void* stream) {
+    if (!b) return fail(UP_ERR_INVALID_ARG, "batch is NULL");
+    for (size_t k = 0; k < b->bound.size(); k++)
+        if (!b->bound[k]) return fail(UP_ERR_INVALID_ARG, "task " + std::to_string(k) + " is not bound");
+    cudaStream_t s = (cudaStream_t)stream;
+    up_status st = prepare(b);
+    if (st != UP_OK) return st;
+    if (b->opts.autotune && !b->tuned) {
+        if ((st = autotune(b, s)) != UP_OK) return st;
+    }
+    if (!b->opts.use_graph) return run_step(b, err_word, s);
+    if (b->gexec && b->graph_err != err_word) b->drop_graph();
+    if (!b->gexec) {
+        cudaGraph_t g = nullptr;
+        UPB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        up_status st2 = run_step(b, err_word, s);
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (st2 != UP_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st2;
+        }
+        if (e != cudaSuccess) return cuda_err(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&b->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_err(e, "cudaGraphInstantiate");
+        b->graph_err = err_word;
+    }
+    UPB_CUDA(cudaGraphLaunch(b->gexec, s));
+    return UP_OK;
+}
+
+up_status up_batch_shape(const up_batch* b, int32_t band, int32_t* block_threads, int32_t* ctas_per_sm,
+                         int32_t* tile_rows, double* tuned_ms) {
+    if (!b || band < 0 || band > 2) return fail(UP_ERR_INVALID_ARG, "bad band");
+    const Shape& s = b->shape[band];
+    if (block_threads) *block_threads = kThreads[s.threads_idx];
+    if (ctas_per_sm) *ctas_per_sm = s.ctas_per_sm;
+    if (tile_rows) *tile_rows = s.tile_rows;
+    if (tuned_ms) *tuned_ms = s.tuned_ms;
+    return UP_OK;
+}
+
+up_status up_batch_task_type(const up_batch* b, int32_t task, int32_t* precision, int32_t* scale,
+                             int32_t* value_bytes, int32_t* band) {
+    if (!b || task < 0 || task >= (int)b->gen.tasks.size()) return fail(UP_ERR_INVALID_ARG, "bad task");
+    const auto& t = b->gen.tasks[task];
+    if (precision) *precision = t.out_p;
+    if (scale) *scale = t.out_s;
+    if (value_bytes) *value_bytes = t.out_bytes;
+    if (band) *band = t.band;
+    return UP_OK;
+}
+
+void up_batch_release(up_batch* b) { delete b; }
+
+up_status up_util_compile_batch_only(const up_batch_task* tasks, int32_t n_tasks) {
+    if (!tasks || n_tasks <= 0) return fail(UP_ERR_INVALID_ARG, "no tasks");
+    std::vector<BatchTaskDesc> desc(n_tasks);
+    for (int k = 0; k < n_tasks; k++)
+        desc[k] = BatchTaskDesc{tasks[k].nodes, tasks[k].n_nodes, tasks[k].root, tasks[k].cols, tasks[k].n_cols,
+                                tasks[k].agg_kind};
+    GeneratedBatch gen;
+    up_status st = generate_batch_module(desc.data(), n_tasks, gen);
+    if (st != UP_OK) return st;
+    std::vector<char> cubin;
+    return jit_compile_linked(gen.units, cubin);
+}
+
+}  // extern "C"

@@ -569,3 +569,205 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
 }
 
 }  // namespace upi
+
+namespace upi {
+
+// ----------------------------------------------------- batch modules
+// Each distinct task becomes one relocatable unit whose functions are named
+// by a hash of their body (so a unit compiled once is reused by every batch
+// that contains the same task); a dispatcher unit holds, per precision band,
+// a persistent kernel (in three block sizes) that pulls (task, tile) work
+// items and calls the task's tile function, plus the finalisation kernel.
+namespace {
+const char* kBatchPrelude =
+    "#define UP_MUL_UNROLL_PAIRS 1024\n"
+    "#include \"up_dev.cuh\"\nusing namespace up;\n"
+    "struct BTask { KCol col[8]; i64 rows; u8* out; const int* gid; u32* acc; u64* cnt; int n_groups; int words; };\n"
+    "struct BArgs { BTask* tasks; const int* item_task; const i64* item_tile; i64 n_items; "
+    "unsigned long long* head; u32* err; int tile_rows; int pad; };\n";
+
+uint64_t text_hash(const std::string& s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+std::string replace_all(std::string s, const std::string& from, const std::string& to) {
+    size_t p = 0;
+    while ((p = s.find(from, p)) != std::string::npos) {
+        s.replace(p, from.size(), to);
+        p += to.size();
+    }
+    return s;
+}
+}  // namespace
+
+up_status generate_batch_module(const BatchTaskDesc* tasks, int n_tasks, GeneratedBatch& out) {
+    if (n_tasks <= 0 || n_tasks > 1024) return fail(UP_ERR_INVALID_ARG, "1..1024 tasks");
+    out.tasks.assign(n_tasks, GeneratedBatch::Task());
+    out.units.clear();
+    std::vector<std::string> fname(n_tasks);
+    std::map<std::string, int> unit_of;
+    for (int k = 0; k < n_tasks; k++) {
+        const BatchTaskDesc& t = tasks[k];
+        if (t.n_cols < 1 || t.n_cols > 8) return fail(UP_ERR_INVALID_ARG, "tasks take 1..8 columns");
+        std::vector<NodeFacts> f;
+        std::vector<int> topo;
+        up_status st = analyze_nodes(t.nodes, t.n_nodes, t.cols, t.n_cols, f, topo, {t.root});
+        if (st != UP_OK) return st;
+        GeneratedBatch::Task& gt = out.tasks[k];
+        int max_limbs = 1;
+        for (int n : topo) max_limbs = std::max(max_limbs, f[n].limbs);
+        if (max_limbs > 128) return fail(UP_ERR_UNSUPPORTED, "task " + std::to_string(k) + " wider than 4096 bits");
+        gt.band = max_limbs <= 4 ? 0 : (max_limbs <= 24 ? 1 : 2);
+        gt.agg = t.agg_kind;
+        const up_expr_node& rn = t.nodes[t.root];
+        const bool cmp_root = is_compare_kind(rn.kind);
+        std::vector<int> used;
+        for (int n : topo)
+            if (t.nodes[n].kind == UP_NODE_COLUMN &&
+                std::find(used.begin(), used.end(), t.nodes[n].column) == used.end())
+                used.push_back(t.nodes[n].column);
+        std::sort(used.begin(), used.end());
+        gt.in_bytes.assign(t.n_cols, 0);
+        for (int c = 0; c < t.n_cols; c++) gt.in_bytes[c] = compact_bytes(t.cols[c].precision);
+        Emitter em(t.nodes, t.cols, f);
+        for (int n : topo) em.node(n);
+        std::ostringstream src;
+        src << kBatchPrelude;
+        if (t.agg_kind < 0) {
+            if (cmp_root) {
+                gt.out_p = 1;
+                gt.out_s = 0;
+                gt.out_bytes = 1;
+            } else {
+                if (rn.precision < 1) return fail(UP_ERR_INVALID_ARG, "task root precision not set");
+                gt.out_p = rn.precision;
+                gt.out_s = f[t.root].scale;
+                gt.out_bytes = compact_bytes(rn.precision);
+            }
+            const int BO = gt.out_bytes;
+            src << "UP_DI u32 row(" << params_decl(used) << "u8* __restrict__ out, const bool words) {\n";
+            src << "    u32 err = 0u;\n" << em.constants() << em.body.str();
+            if (cmp_root) src << "    out[0] = (u8)c" << t.root << ";\n";
+            else src << "    err |= st_compact_bytes<" << BO << ">(out, v" << t.root << ", s" << t.root << ");\n";
+            src << "    return err;\n}\n";
+            src << "extern \"C\" __device__ __noinline__ u32 @@tile(const BTask& t, i64 tile, int tr) {\n";
+            src << "    u32 err = 0u;\n    const i64 r0 = tile * tr;\n";
+            src << "    const i64 r1 = (r0 + tr) < t.rows ? (r0 + tr) : t.rows;\n";
+            src << "    for (i64 r = r0 + threadIdx.x; r < r1; r += blockDim.x) {\n";
+            src << "        const bool words = t.words != 0 && r + 1 < t.rows;  // word reads stay inside the column\n";
+            src << "        err |= row(";
+            for (int c : used) src << "t.col[" << c << "].data + r * " << gt.in_bytes[c] << ", ";
+            src << "t.out + r * " << BO << ", words);\n    }\n    return err;\n}\n";
+        } else {
+            if (cmp_root) return fail(UP_ERR_INVALID_ARG, "cannot aggregate a comparison");
+            const NodeFacts& fr = f[t.root];
+            gt.nacc = limbs_for_bits(fr.bits + 1 + 40);
+            gt.agg_scale = fr.scale;
+            src << "UP_DI u32 qrow(" << params_decl(used) << "u32* __restrict__ acc, const bool words) {\n";
+            src << "    u32 err = 0u;\n" << em.constants() << em.body.str();
+            if (t.agg_kind != UP_AGG_COUNT)
+                src << "    atomic_acc_add<" << gt.nacc << ">(acc, v" << t.root << ", s" << t.root << ");\n";
+            src << "    return err;\n}\n";
+            src << "extern \"C\" __device__ __noinline__ u32 @@tile(const BTask& t, i64 tile, int tr) {\n";
+            src << "    u32 err = 0u;\n    const i64 r0 = tile * tr;\n";
+            src << "    const i64 r1 = (r0 + tr) < t.rows ? (r0 + tr) : t.rows;\n";
+            src << "    for (i64 r = r0 + threadIdx.x; r < r1; r += blockDim.x) {\n";
+            src << "        const int g = t.gid[r];\n";
+            src << "        if ((unsigned)g >= (unsigned)t.n_groups) { err |= ERR_DOMAIN; continue; }\n";
+            src << "        atomicAdd(t.cnt + g, 1ull);\n";
+            if (t.agg_kind != UP_AGG_COUNT) {
+                src << "        const bool words = t.words != 0 && r + 1 < t.rows;\n";
+                src << "        err |= qrow(";
+                for (int c : used) src << "t.col[" << c << "].data + r * " << gt.in_bytes[c] << ", ";
+                src << "t.acc + (i64)g * " << gt.nacc << ", words);\n";
+            }
+            src << "    }\n    return err;\n}\n";
+            src << "extern \"C\" __device__ __noinline__ void @@fin(const BTask& t, int g) {\n";
+            src << "    const u64 cnt = t.cnt[g];\n";
+            if (t.agg_kind == UP_AGG_COUNT) {
+                src << "    ((i64*)t.out)[g] = (i64)cnt;\n";
+            } else {
+                const int n = gt.nacc;
+                src << "    u32 m[" << n << "];\n";
+                src << "    for (int i = 0; i < " << n << "; i++) m[i] = t.acc[(i64)g * " << n << " + i];\n";
+                src << "    const u32 neg = m[" << n - 1 << "] >> 31;\n    if (neg) negate(m);\n";
+                src << "    u8* img = t.out + (i64)g * 133;\n";
+                if (t.agg_kind == UP_AGG_SUM) {
+                    src << "    agg_image(img, cnt > 0 ? 1u : 0u, neg, " << gt.agg_scale << "u, m);\n";
+                } else {
+                    src << "    const u32 P10_4[1] = {10000u};\n";
+                    src << "    if (cnt == 0) { agg_image(img, 0u, 0u, " << gt.agg_scale + 4 << "u, m); return; }\n";
+                    src << "    const u32 c2[2] = {(u32)cnt, (u32)(cnt >> 32)};\n";
+                    src << "    u32 q[" << n + 1 << "]; u32 sq;\n";
+                    src << "    div_round<" << n + 1 << ", " << n << ", 2, 1, 4u, 10000ull>(q, sq, m, neg, c2, 0u, P10_4);\n";
+                    src << "    agg_image(img, 1u, sq, " << gt.agg_scale + 4 << "u, q);\n";
+                }
+            }
+            src << "}\n";
+        }
+        const std::string body = src.str();
+        char hname[40];
+        snprintf(hname, sizeof hname, "ut%016llx_", (unsigned long long)text_hash(body));
+        fname[k] = hname;
+        if (!unit_of.count(hname)) {
+            unit_of[hname] = (int)out.units.size();
+            out.units.push_back(replace_all(body, "@@", hname));
+        }
+    }
+    // dispatcher unit
+    std::ostringstream d;
+    d << kBatchPrelude;
+    std::set<std::string> declared;
+    std::vector<int> aggs;
+    for (int k = 0; k < n_tasks; k++) {
+        if (out.tasks[k].agg >= 0) aggs.push_back(k);
+        if (declared.insert(fname[k]).second) {
+            d << "extern \"C\" __device__ u32 " << fname[k] << "tile(const BTask& t, i64 tile, int tr);\n";
+            if (out.tasks[k].agg >= 0) d << "extern \"C\" __device__ void " << fname[k] << "fin(const BTask& t, int g);\n";
+        }
+    }
+    static const int kThreads[3] = {64, 128, 256};
+    out.kernels.clear();
+    for (int b = 0; b < 3; b++) {
+        std::ostringstream body;
+        body << "    __shared__ i64 s_item;\n    u32 err = 0u;\n";
+        body << "    for (;;) {\n";
+        body << "        if (threadIdx.x == 0) s_item = (i64)atomicAdd(a.head, 1ull);\n";
+        body << "        __syncthreads();\n        const i64 it = s_item;\n        __syncthreads();\n";
+        body << "        if (it >= a.n_items) break;\n";
+        body << "        const int task = a.item_task[it];\n        const i64 tile = a.item_tile[it];\n";
+        body << "        switch (task) {\n";
+        for (int k = 0; k < n_tasks; k++)
+            if (out.tasks[k].band == b)
+                body << "            case " << k << ": err |= " << fname[k] << "tile(a.tasks[" << k
+                     << "], tile, a.tile_rows); break;\n";
+        body << "            default: break;\n        }\n    }\n";
+        body << "    err = __reduce_or_sync(0xffffffffu, err);\n";
+        body << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n";
+        for (int ti = 0; ti < 3; ti++) {
+            std::string name = "up_batch_b" + std::to_string(b) + "_t" + std::to_string(kThreads[ti]);
+            d << "extern \"C\" __global__ void __launch_bounds__(" << kThreads[ti] << ") " << name
+              << "(const BArgs a) {\n" << body.str() << "}\n";
+            out.kernels.push_back(name);
+        }
+    }
+    d << "extern \"C\" __global__ void __launch_bounds__(256) up_batch_fin(const BArgs a) {\n";
+    d << "    const int g = blockIdx.x * blockDim.x + threadIdx.x;\n    switch (blockIdx.y) {\n";
+    for (size_t i = 0; i < aggs.size(); i++)
+        d << "        case " << i << ": if (g < a.tasks[" << aggs[i] << "].n_groups) " << fname[aggs[i]] << "fin(a.tasks["
+          << aggs[i] << "], g); break;\n";
+    d << "        default: break;\n    }\n}\n";
+    out.kernels.push_back("up_batch_fin");
+    out.units.push_back(d.str());
+    out.agg_tasks = aggs;
+    out.source.clear();
+    for (const auto& u : out.units) out.source += u;
+    return UP_OK;
+}
+
+}  // namespace upi

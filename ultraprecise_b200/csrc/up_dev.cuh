@@ -27,6 +27,11 @@ typedef unsigned char u8;
 
 #define UP_DI __device__ __forceinline__
 
+#ifndef UP_MUL_UNROLL_PAIRS
+#define UP_MUL_UNROLL_PAIRS 4096
+#endif
+constexpr int kMulUnrollPairs = UP_MUL_UNROLL_PAIRS;
+
 enum : u32 { ERR_OVERFLOW = 1u, ERR_DIV0 = 2u, ERR_DOMAIN = 4u };
 
 // ----------------------------------------------------------------- limbs
@@ -152,7 +157,9 @@ UP_DI void add_signed(u32 (&r)[N], u32& sr, const u32 (&a)[NA], u32 sa, const u3
 template <int N, int NA, int NB>
 UP_DI void mul(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
     zero(r);
-#pragma unroll
+    // products above UP_MUL_UNROLL_PAIRS limb pairs keep the outer loop rolled
+    // (compile time)
+#pragma unroll((NA * NB <= kMulUnrollPairs) ? NA : 1)
     for (int i = 0; i < NA; i++) {
         if (i >= N) break;
         u64 c = 0;

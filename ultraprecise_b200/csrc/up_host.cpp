@@ -1,4 +1,6 @@
 // up_host.cpp — errors, layout tables, host big integers and node analysis.
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -220,6 +222,10 @@ Big big_from_dec(const std::string& s) {
     }
     big_trim(r);
     return r;
+}
+
+void mkdir_if_missing(const std::string& dir) {
+    if (!dir.empty()) mkdir(dir.c_str(), 0755);
 }
 
 // ------------------------------------------------------ node analysis

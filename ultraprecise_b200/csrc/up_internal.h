@@ -76,6 +76,31 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
                                 const up_query_agg* aggs, int n_aggs, const up_compile_opts* opts,
                                 GeneratedModule& out);
 
+// batch modules (one source, every task; persistent band kernels)
+struct BatchTaskDesc {
+    const up_expr_node* nodes;
+    int n_nodes;
+    int root;
+    const up_col_type* cols;
+    int n_cols;
+    int agg_kind;  // -1 projection
+};
+struct GeneratedBatch {
+    struct Task {
+        int band = 0;
+        int agg = -1;
+        int out_p = 0, out_s = 0, out_bytes = 0;
+        int nacc = 0, agg_scale = 0;
+        std::vector<int> in_bytes;
+    };
+    std::vector<Task> tasks;
+    std::vector<int> agg_tasks;
+    std::vector<std::string> units;  // one relocatable unit per distinct task, then the dispatcher
+    std::string source;              // all units concatenated (cache key of the batch)
+    std::vector<std::string> kernels;
+};
+up_status generate_batch_module(const BatchTaskDesc* tasks, int n_tasks, GeneratedBatch& out);
+
 // ------------------------------------------------------------------ JIT
 struct JitKernelSet;  // opaque: loaded library + kernel handles
 struct JitModule {
@@ -84,6 +109,9 @@ struct JitModule {
 };
 // Compile (or fetch from the cache) and load.  Thread-safe.
 up_status jit_compile_cubin(const std::string& src, std::vector<char>& cubin);
+up_status jit_compile_linked(const std::vector<std::string>& units, std::vector<char>& linked);
+up_status jit_load(const std::vector<char>& cubin, const std::vector<std::string>& kernels,
+                   std::shared_ptr<JitKernelSet>& out);
 up_status jit_get(const GeneratedModule& gen, std::shared_ptr<JitKernelSet>& out);
 void* jit_kernel(const JitKernelSet& ks, const std::string& name);  // cudaKernel_t as void*
 int jit_cache_size(bool clear);
@@ -91,6 +119,7 @@ const std::string& device_header_source();
 
 // ------------------------------------------------------------ devices
 int sm_count_current();
+void mkdir_if_missing(const std::string& dir);
 
 }  // namespace upi
 

@@ -10,6 +10,7 @@
 // context-independent cudaLibraryLoadData, whose kernel handles are valid on
 // every device of the process.
 #include <cuda_runtime.h>
+#include <nvJitLink.h>
 #include <nvrtc.h>
 #include <dlfcn.h>
 #include <sys/stat.h>
@@ -18,10 +19,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <atomic>
 #include <list>
 #include <map>
 #include <mutex>
 #include <sstream>
+#include <thread>
 #include <unordered_map>
 
 #include "up_internal.h"
@@ -94,10 +97,11 @@ void mkdirs(const std::string& path) {
     }
 }
 
-std::string full_key(const std::string& src) {
+std::string full_key(const std::string& src, bool rdc) {
     int maj = 0, min = 0;
     nvrtcVersion(&maj, &min);
-    return std::string(kArch) + "|nvrtc" + std::to_string(maj) + "." + std::to_string(min) + "|" + src;
+    return std::string(kArch) + (rdc ? "|rdc" : "") + "|nvrtc" + std::to_string(maj) + "." + std::to_string(min) +
+           "|" + src;
 }
 
 bool read_file(const std::string& p, std::string& out) {
@@ -119,14 +123,14 @@ void write_file_atomic(const std::string& p, const std::string& data) {
     rename(tmp.c_str(), p.c_str());
 }
 
-up_status nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::string& log) {
+up_status nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::string& log, bool rdc) {
     nvrtcProgram prog;
     const char* hdr_src[1] = {device_header_source().c_str()};
     const char* hdr_name[1] = {"up_dev.cuh"};
     nvrtcResult r = nvrtcCreateProgram(&prog, src.c_str(), "up_kernel.cu", 1, hdr_src, hdr_name);
     if (r != NVRTC_SUCCESS) return fail(UP_ERR_COMPILE, std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r));
-    const char* opts[] = {kArch, "-std=c++17", "-lineinfo", "--restrict", "-DUP_NVRTC=1"};
-    r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+    const char* opts[] = {kArch, "-std=c++17", "-lineinfo", "--restrict", "-DUP_NVRTC=1", "-rdc=true"};
+    r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])) - (rdc ? 0 : 1), opts);
     size_t ls = 0;
     nvrtcGetProgramLogSize(prog, &ls);
     log.assign(ls, '\0');
@@ -161,8 +165,10 @@ Cache& cache() {
 
 }  // namespace
 
-up_status jit_compile_cubin(const std::string& src, std::vector<char>& cubin) {
-    const std::string key = full_key(src);
+// Compile (or read from the disk cache) one source to a CUBIN; with rdc the
+// CUBIN is relocatable, for linking with others by nvJitLink.
+up_status jit_compile_unit(const std::string& src, bool rdc, std::vector<char>& cubin) {
+    const std::string key = full_key(src, rdc);
     const uint64_t h = fnv1a(key);
     char name[32];
     snprintf(name, sizeof name, "%016llx", (unsigned long long)h);
@@ -176,13 +182,148 @@ up_status jit_compile_cubin(const std::string& src, std::vector<char>& cubin) {
         }
     }
     std::string log;
-    up_status st = nvrtc_compile(src, cubin, log);
+    up_status st = nvrtc_compile(src, cubin, log, rdc);
     if (st != UP_OK) return st;
     if (disk_cache_enabled()) {
         mkdirs(dir);
         write_file_atomic(base + ".cubin", std::string(cubin.begin(), cubin.end()));
         write_file_atomic(base + ".key", key);
     }
+    return UP_OK;
+}
+
+up_status jit_compile_cubin(const std::string& src, std::vector<char>& cubin) {
+    return jit_compile_unit(src, false, cubin);
+}
+
+// nvJitLink is resolved at run time from the CUDA toolkit by absolute path
+// (another copy with the same soname may already be loaded by a framework),
+// under the versioned names its header maps the API to.
+#define UP_STR2(x) #x
+#define UP_STR(x) UP_STR2(x)
+struct JitLinkApi {
+    decltype(&nvJitLinkCreate) create = nullptr;
+    decltype(&nvJitLinkAddData) add = nullptr;
+    decltype(&nvJitLinkComplete) complete = nullptr;
+    decltype(&nvJitLinkGetLinkedCubinSize) cubin_size = nullptr;
+    decltype(&nvJitLinkGetLinkedCubin) cubin = nullptr;
+    decltype(&nvJitLinkGetErrorLogSize) log_size = nullptr;
+    decltype(&nvJitLinkGetErrorLog) log = nullptr;
+    decltype(&nvJitLinkDestroy) destroy = nullptr;
+    bool ok = false;
+};
+
+const JitLinkApi& jitlink() {
+    static JitLinkApi api = [] {
+        JitLinkApi a;
+        std::vector<std::string> paths;
+        if (const char* ch = getenv("CUDA_HOME")) paths.push_back(std::string(ch) + "/lib64/libnvJitLink.so.12");
+        paths.push_back("/usr/local/cuda/lib64/libnvJitLink.so.12");
+        paths.push_back("libnvJitLink.so.12");
+        void* h = nullptr;
+        for (const auto& p : paths)
+            if ((h = dlopen(p.c_str(), RTLD_NOW | RTLD_LOCAL))) break;
+        if (!h) return a;
+        a.create = (decltype(a.create))dlsym(h, UP_STR(nvJitLinkCreate));
+        a.add = (decltype(a.add))dlsym(h, UP_STR(nvJitLinkAddData));
+        a.complete = (decltype(a.complete))dlsym(h, UP_STR(nvJitLinkComplete));
+        a.cubin_size = (decltype(a.cubin_size))dlsym(h, UP_STR(nvJitLinkGetLinkedCubinSize));
+        a.cubin = (decltype(a.cubin))dlsym(h, UP_STR(nvJitLinkGetLinkedCubin));
+        a.log_size = (decltype(a.log_size))dlsym(h, UP_STR(nvJitLinkGetErrorLogSize));
+        a.log = (decltype(a.log))dlsym(h, UP_STR(nvJitLinkGetErrorLog));
+        a.destroy = (decltype(a.destroy))dlsym(h, UP_STR(nvJitLinkDestroy));
+        a.ok = a.create && a.add && a.complete && a.cubin_size && a.cubin && a.log_size && a.log && a.destroy;
+        return a;
+    }();
+    return api;
+}
+
+// Compile every unit (relocatable, cached per unit, in parallel) and link
+// them with nvJitLink; the linked CUBIN is cached under the units' keys.
+up_status jit_compile_linked(const std::vector<std::string>& units, std::vector<char>& linked) {
+    std::string all;
+    for (const auto& u : units) all += full_key(u, true) + "\x1f";
+    const std::string key = "linked|" + all;
+    char name[40];
+    snprintf(name, sizeof name, "L%016llx", (unsigned long long)fnv1a(key));
+    const std::string base = cache_dir() + "/" + name;
+    if (disk_cache_enabled()) {
+        std::string k2, bin;
+        if (read_file(base + ".key", k2) && k2 == key && read_file(base + ".cubin", bin) && !bin.empty()) {
+            linked.assign(bin.begin(), bin.end());
+            return UP_OK;
+        }
+    }
+    std::vector<std::vector<char>> objs(units.size());
+    std::vector<up_status> sts(units.size(), UP_OK);
+    std::vector<std::string> errs(units.size());
+    {
+        unsigned nthr = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 32u));
+        std::vector<std::thread> pool;
+        std::atomic<size_t> next{0};
+        for (unsigned t = 0; t < nthr; t++)
+            pool.emplace_back([&]() {
+                for (size_t i; (i = next.fetch_add(1)) < units.size();) {
+                    sts[i] = jit_compile_unit(units[i], true, objs[i]);
+                    if (sts[i] != UP_OK) errs[i] = last_error();
+                }
+            });
+        for (auto& th : pool) th.join();
+    }
+    for (size_t i = 0; i < units.size(); i++)
+        if (sts[i] != UP_OK) return fail(sts[i], "unit " + std::to_string(i) + ": " + errs[i]);
+    const JitLinkApi& L = jitlink();
+    if (!L.ok) return fail(UP_ERR_COMPILE, "libnvJitLink.so.12 not found (needed to link batch modules)");
+    nvJitLinkHandle h;
+    const char* lopts[] = {"-arch=sm_100a"};
+    if (L.create(&h, 1, lopts) != NVJITLINK_SUCCESS) return fail(UP_ERR_COMPILE, "nvJitLinkCreate failed");
+    nvJitLinkResult lr = NVJITLINK_SUCCESS;
+    for (size_t i = 0; i < objs.size() && lr == NVJITLINK_SUCCESS; i++)
+        lr = L.add(h, NVJITLINK_INPUT_CUBIN, objs[i].data(), objs[i].size(), ("unit" + std::to_string(i)).c_str());
+    if (lr == NVJITLINK_SUCCESS) lr = L.complete(h);
+    if (lr != NVJITLINK_SUCCESS) {
+        size_t ls = 0;
+        L.log_size(h, &ls);
+        std::string log(ls, '\0');
+        if (ls) L.log(h, &log[0]);
+        L.destroy(&h);
+        return fail(UP_ERR_COMPILE, "nvJitLink: " + log);
+    }
+    size_t n = 0;
+    L.cubin_size(h, &n);
+    linked.resize(n);
+    L.cubin(h, linked.data());
+    L.destroy(&h);
+    if (disk_cache_enabled()) {
+        mkdirs(cache_dir());
+        write_file_atomic(base + ".cubin", std::string(linked.begin(), linked.end()));
+        write_file_atomic(base + ".key", key);
+    }
+    return UP_OK;
+}
+
+// Load an already compiled CUBIN and look up its kernels.
+up_status jit_load(const std::vector<char>& cubin, const std::vector<std::string>& kernels,
+                   std::shared_ptr<JitKernelSet>& out) {
+    auto ks = std::make_shared<JitKernelSet>();
+    ks->cubin = cubin;
+    cudaError_t e = cudaLibraryLoadData(&ks->lib, ks->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e != cudaSuccess) {
+        ks->lib = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? UP_ERR_NO_DEVICE : UP_ERR_CUDA,
+                    std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e));
+    }
+    for (const auto& k : kernels) {
+        cudaKernel_t h = nullptr;
+        e = cudaLibraryGetKernel(&h, ks->lib, k.c_str());
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(UP_ERR_CUDA, "cudaLibraryGetKernel(" + k + "): " + cudaGetErrorString(e));
+        }
+        ks->kernels[k] = h;
+    }
+    out = ks;
     return UP_OK;
 }
 

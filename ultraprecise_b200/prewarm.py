@@ -33,6 +33,11 @@ def prewarm(verbose: bool = False) -> None:
                 print("prewarmed", p, op)
     exprs, aggs, cols = workloads.query_exprs()
     _compile(exprs, cols, aggs)
+    from . import batch
+    tasks, _ = workloads.batch_tasks()
+    batch.compile_only(workloads.batch_specs(tasks))
+    if verbose:
+        print("prewarmed batch module,", len(tasks), "tasks")
 
 
 if __name__ == "__main__":

@@ -38,3 +38,69 @@ def query_exprs():
     aggs = [(abi.UP_AGG_SUM, 0), (abi.UP_AGG_SUM, 1), (abi.UP_AGG_SUM, 2), (abi.UP_AGG_SUM, 3),
             (abi.UP_AGG_AVG, 0), (abi.UP_AGG_AVG, 1), (abi.UP_AGG_AVG, 4), (abi.UP_AGG_COUNT, 0)]
     return exprs, aggs, cols
+
+
+# Batched mixed precision: 64 tasks, random trees of depth 3-5 over +,-,*,/ on
+# 2-4 columns; p log-uniform in [10,400], s uniform in [0,p/2], rows
+# log-uniform in [1e3,1e7]; half the tasks end in a grouped SUM over Zipf(1.1)
+# int32 keys with 1..100k groups.  Every node of this path is exact (never
+# truncated), so trees whose intermediates would exceed 4096 bits are redrawn.
+BATCH_MAX_BITS = 4096
+
+
+def _bits_bound(e, s: int, nbytes: int):
+    """(bits, scale) bound of an expression over DECIMAL(p,s) columns, the
+    same bound the library's node analysis computes."""
+    if e.kind == abi.UP_NODE_COLUMN:
+        return 8 * nbytes - 1, s
+    a_bits, a_s = _bits_bound(e.left, s, nbytes)
+    b_bits, b_s = _bits_bound(e.right, s, nbytes)
+    if e.kind in (abi.UP_NODE_ADD, abi.UP_NODE_SUB):
+        sc = max(a_s, b_s)
+        ab = a_bits + ((10 ** (sc - a_s)).bit_length() if sc > a_s else 0)
+        bb = b_bits + ((10 ** (sc - b_s)).bit_length() if sc > b_s else 0)
+        return max(ab, bb) + 1, sc
+    if e.kind == abi.UP_NODE_MUL:
+        return a_bits + b_bits, a_s + b_s
+    return max(64, a_bits + (10 ** (b_s + 4)).bit_length()), a_s + 4
+
+
+def batch_tasks(seed: int = 20261203, n: int = 64, max_bits: int = BATCH_MAX_BITS, row_scale: float = 1.0):
+    """Deterministic task list: dicts with expr, cols, p, s, rows, agg, groups."""
+    import math
+    import random
+    from . import codec
+    rng = random.Random(seed)
+    ops = [abi.UP_NODE_ADD, abi.UP_NODE_SUB, abi.UP_NODE_MUL, abi.UP_NODE_DIV]
+    out = []
+    redraws = 0
+    while len(out) < n:
+        p = int(round(math.exp(rng.uniform(math.log(10), math.log(400)))))
+        s = rng.randint(0, p // 2)
+        rows = max(1, int(round(math.exp(rng.uniform(math.log(1e3), math.log(1e7))) * row_scale)))
+        ncols = rng.randint(2, 4)
+        depth = rng.randint(3, 5)
+
+        def tree(d, must):
+            if d == 0 or (not must and rng.random() < 0.35):
+                return E.col(rng.randrange(ncols))
+            op = rng.choice(ops)
+            deep = rng.randrange(2)
+            return E.Expr(op, tree(d - 1, must and deep == 0), tree(d - 1, must and deep == 1))
+
+        e = tree(depth, True)
+        bits, _ = _bits_bound(e, s, codec.compact_bytes(p))
+        if bits > max_bits:
+            redraws += 1
+            continue
+        agg = abi.UP_AGG_SUM if len(out) % 2 == 0 else -1
+        groups = max(1, int(round(math.exp(rng.uniform(0, math.log(1e5)))))) if agg >= 0 else 0
+        out.append({"expr": e, "cols": [E.ColType(p, s)] * ncols, "p": p, "s": s, "rows": rows, "agg": agg,
+                    "groups": groups, "ncols": ncols, "depth": depth})
+    return out, redraws
+
+
+def batch_specs(tasks):
+    """TaskSpecs of batch_tasks() output."""
+    from .batch import TaskSpec
+    return [TaskSpec(t["expr"], t["cols"], t["agg"]) for t in tasks]
