@@ -1,7 +1,7 @@
 """Benchmark of the exact-decimal path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sweep|query]
+                    [--workload sweep|batch]
 
 Workload "sweep" (default) is the precision sweep: element-wise a*b+c and a/b
 (scale s+4, half-up) on DECIMAL(p, p/4), p in {18,38,76,150,300,600}, every
@@ -10,8 +10,12 @@ halved per doubling of p.  One step = one pass over all twelve
 (p, expression) launches; inputs are resident in HBM and every case's input
 is larger than L2 (126 MB), so no L2 flush is needed between steps.
 
-Workload "query" is the grouped-aggregate query (4 DECIMAL(15,2) columns,
-two CHAR(1) keys, SUM x4 / AVG x3 / COUNT) at 256M rows.
+Workload "batch" is the batched mixed-precision set: 64 seeded tasks (random
++,-,*,/ trees of depth 3-5 on 2-4 DECIMAL(p,s) columns, p log-uniform in
+[10,400], rows log-uniform in [1e3,1e7], half ending in a grouped SUM over
+Zipf(1.1) keys) run as one captured graph of persistent band kernels, beside
+the same 64 tasks launched one by one through the plain per-task path.  A
+step is one pass over all 64 tasks; inputs total about 7.5 GB, larger than L2.
 
 The reference arm (--impl reference) times the CPU restatement of the
 reference's decimal path (oracle/, the reference has no CPU decimal path of
@@ -41,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "query"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -296,6 +300,218 @@ def e2e_ours(args, cases, mods, world, stream):
             "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": steps}
 
 
+# ------------------------------------------------------------ batch workload
+BATCH_METRIC = "queries/s (64-task batched mixed-precision set, graph-replayed persistent kernels), bit-exact"
+
+
+def batch_setup(rank):
+    from ultraprecise_b200 import codec, workloads
+    tasks, redraws = workloads.batch_tasks()
+    for t in tasks:
+        nb = codec.compact_bytes(t["p"])
+        t["madds_per_row"], _, _ = workloads.expr_madds(t["expr"], t["s"], nb)
+        t["in_bytes_per_row"] = t["ncols"] * nb
+    return tasks, redraws
+
+
+def run_batch(args, rank, world):
+    import torch
+    from ultraprecise_b200 import abi, batch, runtime, workloads
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = abi.load()
+    stream = torch.cuda.Stream()
+    tasks, redraws = batch_setup(rank)
+    hbm_peak, peak_kind = peaks()
+    madd_peak = C.c_double(0)
+    abi.check(lib.up_util_imad_peak(C.byref(madd_peak), stream.cuda_stream), "imad peak")
+    specs = workloads.batch_specs(tasks)
+    t_build = time.perf_counter()
+    b = batch.Batch(specs, autotune=True, use_graph=True)
+    build_s = time.perf_counter() - t_build
+    with torch.cuda.stream(stream):
+        data = workloads.batch_columns(tasks, seed=20261203 + 1000003 * rank)
+    torch.cuda.synchronize()
+    outs, gids, devcols = [], [], []
+    out_bytes = 0
+    for k, (t, (rows, cols, gid)) in enumerate(zip(tasks, data)):
+        dc = [runtime.DeviceColumn(c, t["p"], t["s"]) for c in cols]
+        devcols.append(dc)
+        if t["agg"] < 0:
+            vb = b.task_type(k)[2]
+            t["out_bytes_per_row"] = vb
+            o = torch.empty(max(1, rows * vb), dtype=torch.uint8, device="cuda")
+            b.bind(k, dc, rows, o)
+            gids.append(None)
+        else:
+            t["out_bytes_per_row"] = 4  # the group id read
+            g = torch.from_numpy(gid).cuda()
+            o = torch.empty(t["groups"] * abi.UP_AGG_DECIMAL_BYTES, dtype=torch.uint8, device="cuda")
+            b.bind(k, dc, rows, o, g, t["groups"])
+            gids.append(g)
+        out_bytes += o.numel()
+        outs.append(o)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    t_tune = time.perf_counter()
+    b.launch(err, stream=stream)  # tunes (or loads the tuned shapes) and captures the graph
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t_tune
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), world) / steps
+
+    with ClockSampler(dev) as clk:
+        ms_batch = timed(lambda: b.launch(err, stream=stream), args.steps, args.warmup)
+    clocks = clk.summary()
+
+    # the same 64 tasks, one plain launch each (no synchronisation between them)
+    plain = []
+    for t in tasks:
+        if t["agg"] < 0:
+            plain.append(runtime.compile_expr(t["expr"], t["cols"]))
+        else:
+            plain.append(runtime.compile_query([t["expr"]], [(t["agg"], 0)], t["cols"]))
+    plain_out = [torch.empty_like(o) for o in outs]
+
+    def plain_step():
+        for k, (t, m) in enumerate(zip(tasks, plain)):
+            if t["agg"] < 0:
+                m.launch(devcols[k], data[k][0], out=plain_out[k], err=err, stream=stream)
+            else:
+                m.launch(devcols[k], gids[k], t["groups"], outs=[plain_out[k]], err=err, stream=stream)
+
+    ms_plain = timed(plain_step, max(1, min(args.steps, 5)), max(1, min(args.warmup, 3)))
+    torch.cuda.synchronize()
+    same = all(torch.equal(a, c) for a, c in zip(outs, plain_out))
+
+    rows = sum(t["rows"] for t in tasks)
+    bytes_step = sum(t["rows"] * (t["in_bytes_per_row"] + t["out_bytes_per_row"]) for t in tasks)
+    madds_step = sum(t["rows"] * t["madds_per_row"] for t in tasks)
+    gmadds = madds_step / (ms_batch * 1e-3) / 1e9
+    gbs = bytes_step / (ms_batch * 1e-3) / 1e9
+    n = len(tasks)
+    shapes = {f"band{i}": b.shape(i) for i in range(3)}
+    res = {"metric": BATCH_METRIC, "value": round(n * world / (ms_batch * 1e-3), 2), "unit": "queries/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_batch, 4),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+           "config": {"workload": "64-task batched mixed precision (seeded trees, p 10-400, rows 1e3-1e7, half "
+                                  "grouped SUM over Zipf(1.1) keys)", "rows_per_step_per_gpu": rows,
+                      "tree_redraws": redraws, "l2": "inputs larger than L2 (no flush)",
+                      "parallelism": f"replicas x{world} (no collective)"},
+           "rows_per_s": round(rows * world / (ms_batch * 1e-3)),
+           "plain": {"ms_per_step": round(ms_plain, 4), "queries_per_s": round(n * world / (ms_plain * 1e-3), 2),
+                     "speedup_batched": round(ms_plain / ms_batch, 3), "byte_equal": same},
+           "roofline": {"bound": "int32", "achieved": round(gmadds, 1), "peak": round(madd_peak.value / 1e9, 1),
+                        "unit": "G limb-madd/s", "frac": round(gmadds * 1e9 / madd_peak.value, 4),
+                        "traffic": None, "kernel": "up_batch band kernels (whole graph)",
+                        "peak_source": "measured (up_util_imad_peak)", "hbm_achieved_gbs": round(gbs, 1),
+                        "hbm_frac": round(gbs / hbm_peak, 4)},
+           "shapes": shapes, "module_build_s": round(build_s, 2), "tune_and_capture_s": round(tune_s, 2),
+           "gpu_launches": args.steps * (1 + sum(1 for i in range(3) if any(
+               b.task_type(k)[3] == i for k in range(n)))), "clocks": clocks}
+    if not args.no_e2e:
+        res["e2e"] = e2e_batch(args, b, tasks, data, outs, gids, world, stream)
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        res["cpu_baseline"] = cpu_baseline_batch(tasks, args.cpu_seconds)
+    return res
+
+
+def e2e_batch(args, b, tasks, data, outs, gids, world, stream):
+    """The batch through its public API with HOST buffers: per step every
+    task's columns and group ids are copied from pinned host memory into the
+    bound device buffers, the graph runs, and every result is copied back."""
+    import torch
+    pairs_in, pairs_out = [], []
+    for k, (rows, cols, _) in enumerate(data):
+        for c in cols:
+            h = torch.empty(c.numel(), dtype=torch.uint8, pin_memory=True)
+            h.copy_(c)
+            pairs_in.append((c, h))
+        if gids[k] is not None:
+            h = torch.empty(gids[k].numel(), dtype=torch.int32, pin_memory=True)
+            h.copy_(gids[k])
+            pairs_in.append((gids[k], h))
+        pairs_out.append((torch.empty(outs[k].numel(), dtype=torch.uint8, pin_memory=True), outs[k]))
+    h2d = sum(h.numel() * h.element_size() for _, h in pairs_in)
+    d2h = sum(h.numel() for h, _ in pairs_out)
+
+    def step():
+        with torch.cuda.stream(stream):
+            for d, h in pairs_in:
+                d.copy_(h, non_blocking=True)
+            b.launch(None, stream=stream)
+            for h, d in pairs_out:
+                h.copy_(d, non_blocking=True)
+
+    steps = max(1, min(args.steps, 3))
+    step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(t0.elapsed_time(t1), world) / steps
+    return {"value": round(len(tasks) * world / (ms * 1e-3), 2), "unit": "queries/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": steps}
+
+
+def batch_cpu_rate(tasks, cpu_seconds, threads, seed=1):
+    """Oracle time for the 64 tasks on the host cores, every task at one common
+    fraction of its rows, extrapolated to full rows: (queries/s, fraction, rows)."""
+    import numpy as np
+    from oracle import gen, oracle
+    from ultraprecise_b200 import codec, workloads
+    from ultraprecise_b200 import expr as E
+
+    def run(frac):
+        secs, rows_tot = 0.0, 0
+        for k, t in enumerate(tasks):
+            r = max(4, int(t["rows"] * frac))
+            nb = codec.compact_bytes(t["p"])
+            cols = [gen.compact_digits(r, t["p"], nb, seed + 97 * k + c, nonzero=True) for c in range(t["ncols"])]
+            bt = E.build([t["expr"]], t["cols"])
+            E.derive_types(bt)
+            if t["agg"] < 0:
+                ob = codec.compact_bytes(bt.nodes[bt.roots[0]].precision)
+                t0 = time.perf_counter()
+                oracle.eval_expr(bt, bt.roots[0], cols, r, ob, threads=threads)
+            else:
+                g = workloads.batch_group_ids(r, t["groups"], seed + k).tobytes()
+                t0 = time.perf_counter()
+                oracle.query(bt, [(t["agg"], bt.roots[0])], cols, g, r, t["groups"], threads=threads)
+            secs += time.perf_counter() - t0
+            rows_tot += r
+        return secs, rows_tot
+
+    f0 = 1.0 / 4096
+    s0, _ = run(f0)
+    frac = min(1.0 / 8, f0 * cpu_seconds / max(s0, 1e-4))
+    s1, rows = run(frac)
+    return len(tasks) / (s1 / frac), frac, rows
+
+
+def cpu_baseline_batch(tasks, cpu_seconds):
+    threads = os.cpu_count() or 1
+    rate, frac, rows = batch_cpu_rate(tasks, cpu_seconds, threads)
+    return {"value": round(rate, 4), "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"{rows} rows: every task at {frac:.2e} of its rows, time scaled to full rows; oracle on "
+                      f"{threads} host threads"}
+
+
 # ------------------------------------------------------ CPU baseline
 def cpu_rate(cases, cpu_seconds, threads, seed=1):
     """Time the oracle on the host cores over the same sweep mix (every case
@@ -342,6 +558,24 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
+    if args.workload == "batch":
+        tasks, _ = batch_setup(rank)
+        per = args.cpu_seconds / max(1, args.steps)
+        rates, rows, frac = [], 0, 0.0
+        for k in range(max(1, args.steps)):
+            r, frac, rows = batch_cpu_rate(tasks, per, threads, seed=1 + k)
+            rates.append(r)
+        rate = sorted(rates)[len(rates) // 2]
+        return {"metric": BATCH_METRIC, "value": round(rate, 4), "unit": "queries/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(len(tasks) / rate * 1e3, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u32 limbs (exact decimal)", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "64-task batched mixed precision on host cores, bounded sample",
+                           "parallelism": f"{threads} host threads"},
+                "cpu_baseline": {"value": round(rate, 4), "unit": "queries/s", "cores": threads, "kind": "port",
+                                 "sample": f"{rows} rows per step: every task at {frac:.2e} of its rows"},
+                "e2e": {"value": round(rate, 4), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
     cases = sweep_cases()
     per = args.cpu_seconds / max(1, args.steps)
     for _ in range(max(0, min(args.warmup, 1))):
@@ -395,7 +629,7 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    res = run_ours(args, rank, world)
+    res = run_batch(args, rank, world) if args.workload == "batch" else run_ours(args, rank, world)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -112,6 +112,7 @@ struct up_batch {
     cudaGraphExec_t gexec = nullptr;
     uint32_t* graph_err = nullptr;
     cudaStream_t side[2] = {nullptr, nullptr};
+    cudaStream_t cap = nullptr;  // private stream the step is captured on (the caller's may be the legacy stream)
     cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
     std::string key;
     void drop_graph() {
@@ -136,6 +137,7 @@ struct up_batch {
     }
     ~up_batch() {
         drop_device();
+        if (cap) cudaStreamDestroy(cap);
         for (int i = 0; i < 2; i++) {
             if (side[i]) cudaStreamDestroy(side[i]);
             if (join[i]) cudaEventDestroy(join[i]);
@@ -273,6 +275,19 @@ up_status prepare(up_batch* b) {
         if (!b->join[i]) UPB_CUDA(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming));
     }
     if (!b->fork) UPB_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    if (!b->cap) UPB_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+    // Task functions are called (not inlined), so wide bands keep their limb
+    // arrays in a stack frame of a few KB per thread; the linker sizes it
+    // statically, and the context's per-thread stack limit is raised to match.
+    size_t need = 0;
+    for (const auto& name : b->gen.kernels) {
+        void* k = jit_kernel(*b->ks, name);
+        cudaFuncAttributes fa;
+        if (k && cudaFuncGetAttributes(&fa, (const void*)k) == cudaSuccess) need = std::max(need, fa.localSizeBytes);
+    }
+    size_t have = 0;
+    UPB_CUDA(cudaDeviceGetLimit(&have, cudaLimitStackSize));
+    if (need > have) UPB_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, (need + 255) & ~size_t(255)));
     for (int band = 0; band < 3; band++) {
         up_status st = build_items(b, band, b->shape[band].tile_rows);
         if (st != UP_OK) return st;
@@ -466,9 +481,9 @@ up_status up_batch_launch(up_batch* b, uint32_t* err_word, void* stream) {
     if (b->gexec && b->graph_err != err_word) b->drop_graph();
     if (!b->gexec) {
         cudaGraph_t g = nullptr;
-        UPB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        up_status st2 = run_step(b, err_word, s);
-        cudaError_t e = cudaStreamEndCapture(s, &g);
+        UPB_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+        up_status st2 = run_step(b, err_word, b->cap);
+        cudaError_t e = cudaStreamEndCapture(b->cap, &g);
         if (st2 != UP_OK) {
             if (g) cudaGraphDestroy(g);
             return st2;

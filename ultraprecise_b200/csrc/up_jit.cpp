@@ -210,6 +210,8 @@ struct JitLinkApi {
     decltype(&nvJitLinkGetErrorLogSize) log_size = nullptr;
     decltype(&nvJitLinkGetErrorLog) log = nullptr;
     decltype(&nvJitLinkDestroy) destroy = nullptr;
+    decltype(&nvJitLinkGetInfoLogSize) info_size = nullptr;
+    decltype(&nvJitLinkGetInfoLog) info = nullptr;
     bool ok = false;
 };
 
@@ -232,6 +234,8 @@ const JitLinkApi& jitlink() {
         a.log_size = (decltype(a.log_size))dlsym(h, UP_STR(nvJitLinkGetErrorLogSize));
         a.log = (decltype(a.log))dlsym(h, UP_STR(nvJitLinkGetErrorLog));
         a.destroy = (decltype(a.destroy))dlsym(h, UP_STR(nvJitLinkDestroy));
+        a.info_size = (decltype(a.info_size))dlsym(h, UP_STR(nvJitLinkGetInfoLogSize));
+        a.info = (decltype(a.info))dlsym(h, UP_STR(nvJitLinkGetInfoLog));
         a.ok = a.create && a.add && a.complete && a.cubin_size && a.cubin && a.log_size && a.log && a.destroy;
         return a;
     }();
@@ -247,7 +251,12 @@ up_status jit_compile_linked(const std::vector<std::string>& units, std::vector<
     char name[40];
     snprintf(name, sizeof name, "L%016llx", (unsigned long long)fnv1a(key));
     const std::string base = cache_dir() + "/" + name;
-    if (disk_cache_enabled()) {
+    // UP_JIT_LINK_VERBOSE=1 relinks and prints the linker's per-kernel
+    // resource report (registers, stack frame, whether the call graph's stack
+    // size could be determined) to stderr.
+    const char* vb = getenv("UP_JIT_LINK_VERBOSE");
+    const bool verbose = vb && *vb && *vb != '0';
+    if (disk_cache_enabled() && !verbose) {
         std::string k2, bin;
         if (read_file(base + ".key", k2) && k2 == key && read_file(base + ".cubin", bin) && !bin.empty()) {
             linked.assign(bin.begin(), bin.end());
@@ -275,8 +284,8 @@ up_status jit_compile_linked(const std::vector<std::string>& units, std::vector<
     const JitLinkApi& L = jitlink();
     if (!L.ok) return fail(UP_ERR_COMPILE, "libnvJitLink.so.12 not found (needed to link batch modules)");
     nvJitLinkHandle h;
-    const char* lopts[] = {"-arch=sm_100a"};
-    if (L.create(&h, 1, lopts) != NVJITLINK_SUCCESS) return fail(UP_ERR_COMPILE, "nvJitLinkCreate failed");
+    const char* lopts[] = {"-arch=sm_100a", "-verbose"};
+    if (L.create(&h, verbose ? 2 : 1, lopts) != NVJITLINK_SUCCESS) return fail(UP_ERR_COMPILE, "nvJitLinkCreate failed");
     nvJitLinkResult lr = NVJITLINK_SUCCESS;
     for (size_t i = 0; i < objs.size() && lr == NVJITLINK_SUCCESS; i++)
         lr = L.add(h, NVJITLINK_INPUT_CUBIN, objs[i].data(), objs[i].size(), ("unit" + std::to_string(i)).c_str());
@@ -288,6 +297,13 @@ up_status jit_compile_linked(const std::vector<std::string>& units, std::vector<
         if (ls) L.log(h, &log[0]);
         L.destroy(&h);
         return fail(UP_ERR_COMPILE, "nvJitLink: " + log);
+    }
+    if (verbose && L.info_size && L.info) {
+        size_t is = 0;
+        L.info_size(h, &is);
+        std::string info(is, '\0');
+        if (is) L.info(h, &info[0]);
+        fprintf(stderr, "%s\n", info.c_str());
     }
     size_t n = 0;
     L.cubin_size(h, &n);

@@ -25,16 +25,30 @@ def _compile(roots, cols, aggs=None):
 
 
 def prewarm(verbose: bool = False) -> None:
+    """Compile every module the benchmarks and GPU tests load, in parallel
+    (the library's compile path releases the GIL and is thread-safe)."""
+    import concurrent.futures as cf
+    import os
+    from . import batch
+    jobs = []
     for p, _ in workloads.SWEEP:
         for op in workloads.SWEEP_OPS:
             e, cols = workloads.sweep_expr(p, op)
-            _compile([e], cols)
-            if verbose:
-                print("prewarmed", p, op)
+            jobs.append((f"sweep p={p} {op}", [e], cols, None))
     exprs, aggs, cols = workloads.query_exprs()
-    _compile(exprs, cols, aggs)
-    from . import batch
+    jobs.append(("query", exprs, cols, aggs))
     tasks, _ = workloads.batch_tasks()
+    # the plain per-task modules the batched mode is compared against
+    for k, t in enumerate(tasks):
+        aggs = None if t["agg"] < 0 else [(t["agg"], 0)]
+        jobs.append((f"batch task {k} plain", [t["expr"]], t["cols"], aggs))
+    workers = max(1, min(32, os.cpu_count() or 1))
+    with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+        futs = {ex.submit(_compile, r, c, a): name for name, r, c, a in jobs}
+        for f in cf.as_completed(futs):
+            f.result()
+            if verbose:
+                print("prewarmed", futs[f])
     batch.compile_only(workloads.batch_specs(tasks))
     if verbose:
         print("prewarmed batch module,", len(tasks), "tasks")

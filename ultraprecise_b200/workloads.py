@@ -104,3 +104,61 @@ def batch_specs(tasks):
     """TaskSpecs of batch_tasks() output."""
     from .batch import TaskSpec
     return [TaskSpec(t["expr"], t["cols"], t["agg"]) for t in tasks]
+
+
+def batch_group_ids(rows: int, groups: int, seed: int):
+    """int32 group ids in [0, groups) drawn from Zipf(1.1) over the group ranks
+    (id 0 is the most frequent), as a numpy array."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    w = np.arange(1, groups + 1, dtype=np.float64) ** -1.1
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    ids = np.searchsorted(cdf, rng.random(rows), side="right")
+    return np.minimum(ids, groups - 1).astype(np.int32)
+
+
+def batch_columns(tasks, seed: int, row_cap: int | None = None):
+    """Device columns and host group ids for batch_tasks() output: per task,
+    its columns (every digit uniform, sign +/-, nonzero values so that leaf
+    divisors are never zero) and, for SUM tasks, Zipf int32 keys.  Returns a
+    list of (rows, [column tensors], group ids numpy array or None)."""
+    from . import runtime
+    out = []
+    for k, t in enumerate(tasks):
+        rows = t["rows"] if row_cap is None else min(t["rows"], row_cap)
+        cols = [runtime.gen_digits(rows, t["p"], seed + 1000 * k + c, signed=True, nonzero=True)
+                for c in range(t["ncols"])]
+        gid = batch_group_ids(rows, t["groups"], seed + 1000 * k + 999) if t["agg"] >= 0 else None
+        out.append((rows, cols, gid))
+    return out
+
+
+def _limbs(bits: int) -> int:
+    return max(1, (bits + 31) // 32)
+
+
+def expr_madds(e, s: int, nbytes: int):
+    """(limb multiply-adds per row, bits, scale) of an expression over
+    DECIMAL(p,s) columns of nbytes each: a*b costs La*Lb, aligning an operand
+    by 10^d costs L*L(10^d), a/b costs the dividend scale-up plus the
+    (m-n+1)*n long-division steps."""
+    if e.kind == abi.UP_NODE_COLUMN:
+        return 0, 8 * nbytes - 1, s
+    am, ab, asc = expr_madds(e.left, s, nbytes)
+    bm, bb, bsc = expr_madds(e.right, s, nbytes)
+    m = am + bm
+    if e.kind in (abi.UP_NODE_ADD, abi.UP_NODE_SUB):
+        sc = max(asc, bsc)
+        if sc > asc:
+            m += _limbs(ab) * _limbs((10 ** (sc - asc)).bit_length())
+        if sc > bsc:
+            m += _limbs(bb) * _limbs((10 ** (sc - bsc)).bit_length())
+    elif e.kind == abi.UP_NODE_MUL:
+        m += _limbs(ab) * _limbs(bb)
+    else:
+        lp = _limbs((10 ** (bsc + 4)).bit_length())
+        la, lb = _limbs(ab), _limbs(bb)
+        m += la * lp + max(1, la + lp - lb + 1) * lb
+    bits, sc = _bits_bound(e, s, nbytes)
+    return m, bits, sc
