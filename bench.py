@@ -1,7 +1,7 @@
 """Benchmark of the exact-decimal path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sweep|batch]
+                    [--workload sweep|batch|query]
 
 Workload "sweep" (default) is the precision sweep: element-wise a*b+c and a/b
 (scale s+4, half-up) on DECIMAL(p, p/4), p in {18,38,76,150,300,600}, every
@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -512,6 +512,171 @@ def cpu_baseline_batch(tasks, cpu_seconds):
                       f"{threads} host threads"}
 
 
+# ------------------------------------------------------------ query workload
+QUERY_METRIC = "decimal rows/s (fused grouped SUM/AVG/COUNT query over DECIMAL(15,2)), bit-exact"
+QUERY_BYTES_PER_ROW = 4 * 7 + 4  # four 7-byte decimal columns and the int32 group id
+
+
+def query_inputs(rows, seed, stream=None):
+    import torch
+    from ultraprecise_b200 import runtime, workloads
+    R = workloads.QUERY_RANGES
+    cols = [runtime.gen_range(rows, 15, *R[n], seed + i, stream=stream) for i, n in enumerate(("qty", "price",
+                                                                                                 "disc", "tax"))]
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    w = torch.tensor([k[2] for k in workloads.QUERY_KEYS], device="cuda")
+    pick = torch.multinomial(w, rows, replacement=True, generator=g) if rows <= (1 << 24) else torch.cat(
+        [torch.multinomial(w, min(1 << 24, rows - o), replacement=True, generator=g) for o in range(0, rows, 1 << 24)])
+    k1 = torch.tensor([k[0][0] for k in workloads.QUERY_KEYS], dtype=torch.uint8, device="cuda")[pick].contiguous()
+    k2 = torch.tensor([k[1][0] for k in workloads.QUERY_KEYS], dtype=torch.uint8, device="cuda")[pick].contiguous()
+    del pick
+    return cols, k1, k2
+
+
+def run_query(args, rank, world):
+    import torch
+    from ultraprecise_b200 import abi, runtime, workloads
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    hbm_peak, peak_kind = peaks()
+    exprs, aggs, ctypes_ = workloads.query_exprs()
+    q = runtime.compile_query(exprs, aggs, ctypes_)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    results = {}
+    for label, rows in (("1M", 1 << 20), ("256M", max(1, int((256 << 20) * args.rows_scale)))):
+        with torch.cuda.stream(stream):
+            cols, k1, k2 = query_inputs(rows, 20261203 + 7 * rank, stream)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            gid, G, _ = runtime.group_ids_from_keys([k1, k2], [1, 1], stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            gid_ms = e0.elapsed_time(e1)
+        dc = [runtime.DeviceColumn(c, 15, 2) for c in cols]
+        outs = [torch.empty(G * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES), dtype=torch.uint8,
+                            device="cuda") for k, _ in aggs]
+
+        def step():
+            q.launch(dc, gid, G, outs=outs, err=err, stream=stream)
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier(world)
+        steps = args.steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
+        gbs = QUERY_BYTES_PER_ROW * rows / (ms * 1e-3) / 1e9
+        results[label] = {"rows": rows, "groups": G, "ms_per_step": round(ms, 4),
+                          "rows_per_s": round(rows * world / (ms * 1e-3)), "hbm_gbs": round(gbs, 1),
+                          "hbm_frac": round(gbs / hbm_peak, 4), "group_ids_ms": round(gid_ms, 3),
+                          "clocks": clk.summary()}
+        if label == "256M":
+            main = results[label]
+            inputs = (cols, k1, k2, gid, G, outs)
+        else:
+            del cols, k1, k2, gid, dc, outs
+    m = main
+    res = {"metric": QUERY_METRIC, "value": m["rows_per_s"], "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+           "config": {"workload": f"grouped SUMx4/AVGx3/COUNT query, DECIMAL(15,2) x4, 2 CHAR(1) keys, "
+                                  f"{m['rows']} rows (256M roofline run; 1M-row case in 'rows_1m')",
+                      "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world} (no collective)"},
+           "roofline": {"bound": "hbm", "achieved": m["hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
+                        "frac": m["hbm_frac"], "traffic": None, "kernel": "up_query_acc + up_query_fin",
+                        "peak_source": peak_kind, "bytes_per_row": QUERY_BYTES_PER_ROW},
+           "rows_1m": results["1M"], "gpu_launches": 2 * args.steps, "clocks": m["clocks"]}
+    if not args.no_e2e:
+        res["e2e"] = e2e_query(args, q, aggs, inputs, world, stream)
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        rate, rows = query_cpu_rate(args.cpu_seconds, os.cpu_count() or 1)
+        res["cpu_baseline"] = {"value": round(rate), "unit": "rows/s", "cores": os.cpu_count() or 1,
+                               "kind": "port", "sample": f"{rows} rows of the same query, oracle on "
+                                                         f"{os.cpu_count() or 1} host threads"}
+    return res
+
+
+def e2e_query(args, q, aggs, inputs, world, stream):
+    """The query through the C ABI with HOST buffers: per step the four
+    decimal columns and the group ids are copied from pinned host memory, the
+    query runs, and the eight aggregate outputs are copied back."""
+    import torch
+    from ultraprecise_b200 import runtime
+    cols, k1, k2, gid, G, outs = inputs
+    pairs = []
+    for d in list(cols) + [gid]:
+        h = torch.empty(d.numel(), dtype=d.dtype, pin_memory=True)
+        h.copy_(d)
+        pairs.append((d, h))
+    hout = [torch.empty(o.numel(), dtype=torch.uint8, pin_memory=True) for o in outs]
+    dc = [runtime.DeviceColumn(c, 15, 2) for c in cols]
+    h2d = sum(h.numel() * h.element_size() for _, h in pairs)
+    d2h = sum(h.numel() for h in hout)
+
+    def step():
+        with torch.cuda.stream(stream):
+            for d, h in pairs:
+                d.copy_(h, non_blocking=True)
+            q.launch(dc, gid, G, outs=outs, stream=stream)
+            for h, o in zip(hout, outs):
+                h.copy_(o, non_blocking=True)
+
+    step()
+    torch.cuda.synchronize()
+    barrier(world)
+    steps = max(1, min(args.steps, 3))
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(t0.elapsed_time(t1), world) / steps
+    rows = gid.numel()
+    return {"value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": steps}
+
+
+def query_cpu_rate(cpu_seconds, threads, seed=3):
+    """Oracle rows/s for the query on the host cores, sized for ~cpu_seconds."""
+    import numpy as np
+    from oracle import gen, oracle
+    from ultraprecise_b200 import workloads
+    from ultraprecise_b200 import expr as E
+    exprs, aggs, ctypes_ = workloads.query_exprs()
+    b = E.build(exprs, ctypes_)
+    E.derive_types(b)
+    qa = [(k, b.roots[i]) for k, i in aggs]
+
+    def run(rows):
+        rng = np.random.default_rng(seed)
+        R = workloads.QUERY_RANGES
+        cols = []
+        for n in ("qty", "price", "disc", "tax"):
+            lo, hi, st = R[n]
+            v = lo + st * rng.integers(0, (hi - lo) // st + 1, rows, dtype=np.int64)
+            cols.append(gen.pack_unsigned(v, 7))
+        w = np.array([k[2] for k in workloads.QUERY_KEYS])
+        g = rng.choice(len(w), size=rows, p=w / w.sum()).astype(np.int32).tobytes()
+        t = time.perf_counter()
+        oracle.query(b, qa, cols, g, rows, len(w), threads=threads)
+        return time.perf_counter() - t
+
+    r0 = 1 << 16
+    s0 = run(r0)
+    rows = int(min(1 << 28, r0 * cpu_seconds / max(s0, 1e-4)))
+    return rows / run(rows), rows
+
+
 # ------------------------------------------------------ CPU baseline
 def cpu_rate(cases, cpu_seconds, threads, seed=1):
     """Time the oracle on the host cores over the same sweep mix (every case
@@ -558,6 +723,21 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
+    if args.workload == "query":
+        per = args.cpu_seconds / max(1, args.steps)
+        rates, rows = [], 0
+        for k in range(max(1, args.steps)):
+            r, rows = query_cpu_rate(per, threads, seed=3 + k)
+            rates.append(r)
+        rate = sorted(rates)[len(rates) // 2]
+        return {"metric": QUERY_METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round((256 << 20) / rate * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+                "impl": "reference", "config": {"workload": "grouped query on host cores, bounded sample",
+                                                "parallelism": f"{threads} host threads"},
+                "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
+                                 "sample": f"{rows} rows per step"},
+                "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "batch":
         tasks, _ = batch_setup(rank)
         per = args.cpu_seconds / max(1, args.steps)
@@ -629,7 +809,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    res = run_batch(args, rank, world) if args.workload == "batch" else run_ours(args, rank, world)
+    run = {"batch": run_batch, "query": run_query}.get(args.workload, run_ours)
+    res = run(args, rank, world)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -30,3 +30,13 @@ def compact_digits(rows: int, p: int, nbytes: int, seed: int, signed: bool = Tru
     if signed:
         raw[:, nbytes - 1] |= (rng.integers(0, 2, size=rows, dtype=np.uint8) << 7).astype(np.uint8)
     return raw.tobytes()
+
+
+def pack_unsigned(values, nbytes: int) -> bytes:
+    """Non-negative int64 values as nbytes-wide little-endian compact decimals
+    (sign bit clear); nbytes <= 8."""
+    v = np.asarray(values, dtype=np.uint64)
+    out = np.zeros((v.size, nbytes), dtype=np.uint8)
+    for i in range(nbytes):
+        out[:, i] = ((v >> np.uint64(8 * i)) & np.uint64(0xFF)).astype(np.uint8)
+    return out.tobytes()

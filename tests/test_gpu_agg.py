@@ -136,3 +136,35 @@ def test_division_int64_matches_oracle():
     for i in range(n):
         exp = oracle.division_int64(bytes(imgs[i * 133:(i + 1) * 133]), counts[i])
         assert got[i * 133:(i + 1) * 133] == exp, i
+
+
+@pytest.mark.parametrize("groups,rows,offset", [
+    (1, 70_001, 0), (3, 5_000, 0), (4, 1_000_000, 0), (4, 100_003, 1), (5, 33_333, 0),
+    (8, 20_000, 0), (9, 20_000, 0), (100, 200_000, 0), (150, 3000, 1), (1000, 50_000, 0),
+    (5000, 300_000, 0), (5000, 7_777, 1)])
+def test_query_accumulation_modes(groups, rows, offset):
+    """Every accumulation strategy of the fused query (per-thread registers,
+    per-CTA shared memory, global) over signed values of three widths; an
+    offset of one row misaligns the columns and group ids, which moves every
+    tile through the synchronous copy path."""
+    cols = [E.ColType(15, 2), E.ColType(30, 5), E.ColType(15, 2)]
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    exprs = [a, a * b, b - c, a * c + b]
+    aggs = [(abi.UP_AGG_SUM, 0), (abi.UP_AGG_SUM, 1), (abi.UP_AGG_AVG, 2), (abi.UP_AGG_COUNT, 0),
+            (abi.UP_AGG_AVG, 0), (abi.UP_AGG_SUM, 3)]
+    q = runtime.compile_query(exprs, aggs, cols)
+    n = rows + offset
+    raw = [runtime.gen_digits(n, ct.precision, 31 * groups + i, signed=True) for i, ct in enumerate(cols)]
+    g = torch.Generator(device="cuda").manual_seed(groups)
+    gid_all = torch.randint(0, groups, (n,), dtype=torch.int32, device="cuda", generator=g)
+    dev = [runtime.DeviceColumn(t[offset * codec.compact_bytes(ct.precision):], ct.precision, ct.scale)
+           for t, ct in zip(raw, cols)]
+    gid = gid_all[offset:]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    outs = q.launch(dev, gid, groups, err=err, rows=rows)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    hraw = [bytes(d.data.cpu().numpy().tobytes()) for d in dev]
+    exp = oracle.query(q.built, q.aggs, hraw, bytes(gid.cpu().numpy().tobytes()), rows, groups, threads=8)
+    for k, (o, e) in enumerate(zip(outs, exp)):
+        assert bytes(o.cpu().numpy().tobytes()) == e, f"aggregate {k}"

@@ -290,11 +290,25 @@ up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64
     a.vec_ok = vec_ok ? 1 : 0;
     void* args[1] = {&a};
     if (e == cudaSuccess && rows > 0) {
-        void* k = jit_kernel(*m->jm.ks, "up_query_acc");
-        const int64_t blocks = (rows + g.block_threads - 1) / g.block_threads;
-        const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, 0) * 4;
-        e = cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(blocks, cap)), dim3(g.block_threads),
-                             args, 0, s);
+        if (contig && g.q_staged) {
+            // staged tiles; accumulators in registers, shared memory or global
+            // memory by group count
+            const char* name = (g.q_gr > 0 && n_groups <= g.q_gr) ? "up_query_tile_r"
+                               : (n_groups <= g.q_gs)             ? "up_query_tile_s"
+                                                                  : "up_query_tile_g";
+            a.vec_ok = (vec_ok && aligned16(group_ids)) ? 1 : 0;
+            void* k = jit_kernel(*m->jm.ks, name);
+            const int64_t ntiles = (rows + g.q_tile_rows - 1) / g.q_tile_rows;
+            const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, g.q_smem);
+            e = cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(ntiles, cap)), dim3(g.block_threads),
+                                 args, (size_t)g.q_smem, s);
+        } else {
+            void* k = jit_kernel(*m->jm.ks, "up_query_acc");
+            const int64_t blocks = (rows + g.block_threads - 1) / g.block_threads;
+            const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, 0) * 4;
+            e = cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(blocks, cap)), dim3(g.block_threads),
+                                 args, 0, s);
+        }
     }
     if (e == cudaSuccess) {
         void* k = jit_kernel(*m->jm.ks, "up_query_fin");

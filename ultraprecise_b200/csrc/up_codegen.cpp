@@ -469,6 +469,9 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     out.agg_scale.clear();
     out.agg_acc_limbs.clear();
     out.agg_acc_offset.clear();
+    // one accumulator per distinct aggregated expression (SUM(x) and AVG(x)
+    // share one), sized for a sign bit and 2^40 rows above the value bound
+    std::vector<int> acc_root, acc_limbs, acc_off;
     int accw = 0;
     for (int a = 0; a < n_aggs; a++) {
         out.agg_kind.push_back(aggs[a].kind);
@@ -478,15 +481,22 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
             out.agg_acc_offset.push_back(0);
             continue;
         }
-        const NodeFacts& fr = f[aggs[a].root];
-        // one sign bit + up to 2^40 rows of headroom above the value bound
+        const int r = aggs[a].root;
+        const NodeFacts& fr = f[r];
         const int nacc = limbs_for_bits(fr.bits + 1 + 40);
+        int slot = (int)(std::find(acc_root.begin(), acc_root.end(), r) - acc_root.begin());
+        if (slot == (int)acc_root.size()) {
+            acc_root.push_back(r);
+            acc_limbs.push_back(nacc);
+            acc_off.push_back(accw);
+            accw += nacc;
+        }
         out.agg_scale.push_back(fr.scale);
         out.agg_acc_limbs.push_back(nacc);
-        out.agg_acc_offset.push_back(accw);
-        accw += nacc;
+        out.agg_acc_offset.push_back(acc_off[slot]);
     }
     out.acc_words_per_group = accw;
+    const int NR = (int)acc_root.size();
 
     Emitter em(nodes, cols, f);
     for (int k : topo) em.node(k);
@@ -494,16 +504,26 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     const int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
     std::ostringstream src;
     src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << kargs_source();
-    src << "UP_DI u32 up_qrow(" << params_decl(used) << "u32* __restrict__ acc, const bool words) {\n";
-    src << "    u32 err = 0u;\n" << em.constants() << em.body.str();
-    for (int a = 0; a < n_aggs; a++) {
-        if (aggs[a].kind == UP_AGG_COUNT) continue;
-        int r = aggs[a].root;
-        src << "    atomic_acc_add<" << out.agg_acc_limbs[a] << ">(acc + " << out.agg_acc_offset[a] << ", v" << r
-            << ", s" << r << ");\n";
-    }
+    // per row: every accumulated expression as a two's complement image
+    src << "UP_DI u32 up_qvals(" << params_decl(used) << "const bool words";
+    for (int i = 0; i < NR; i++) src << ", u32 (&qv" << i << ")[" << acc_limbs[i] << "]";
+    src << ") {\n    u32 err = 0u;\n" << em.constants() << em.body.str();
+    for (int i = 0; i < NR; i++)
+        src << "    to_twos(qv" << i << ", v" << acc_root[i] << ", s" << acc_root[i] << ");\n";
     src << "    return err;\n}\n\n";
+    auto decl_t = [&](const std::string& ind) {
+        std::string d;
+        for (int i = 0; i < NR; i++) d += ind + "u32 qv" + std::to_string(i) + "[" + std::to_string(acc_limbs[i]) + "];\n";
+        return d;
+    };
+    auto targs = [&]() {
+        std::string d;
+        for (int i = 0; i < NR; i++) d += ", qv" + std::to_string(i);
+        return d;
+    };
+    const int W = std::max(accw, 1);
 
+    // generic kernel: blocks, indirection, nullable values; global accumulators
     src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_query_acc(const UpQArgs a) {\n";
     src << "    u32 err = 0u;\n";
     src << "    const i64 stride = (i64)gridDim.x * blockDim.x;\n";
@@ -519,11 +539,178 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
             src << "        else { if (in" << c << "[0] == 0) isnull = true; in" << c << " += 1; }\n";
     }
     src << "        if (isnull) continue;\n";
-    src << "        err |= up_qrow(";
+    src << decl_t("        ");
+    src << "        err |= up_qvals(";
     for (int c : used) src << "in" << c << ", ";
-    src << "a.acc + (i64)g * " << std::max(accw, 1) << ", false);\n    }\n";
+    src << "false" << targs() << ");\n";
+    for (int i = 0; i < NR; i++)
+        src << "        atomic_add_twos(a.acc + (i64)g * " << W << " + " << acc_off[i] << ", qv" << i << ");\n";
+    src << "    }\n";
     src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
     src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
+
+    // Tile kernels (contiguous non-null columns): the decimal columns and the
+    // group ids stream through shared memory by double-buffered bulk copies;
+    // the accumulation strategy depends on the group count (chosen at launch):
+    //   _r  per-thread register accumulators for the first GR groups, merged
+    //       once per thread into shared memory and once per CTA into global;
+    //   _s  per-CTA shared-memory accumulators (up to GS groups), merged once
+    //       per CTA into global;
+    //   _g  global accumulators (many groups: little contention).
+    int row_bytes = 4;
+    for (int c : used) row_bytes += compact_bytes(cols[c].precision);
+    int R = 1024;
+    while (R > 128 && 2L * R * row_bytes > 32 * 1024) R /= 2;
+    const bool staged = 2L * R * row_bytes <= 32 * 1024;
+    int GR = 0;
+    while (GR < 8 && (GR + 1) * (accw + 1) <= 96) GR++;
+    out.q_staged = staged;
+    out.q_tile_rows = R;
+    out.q_gr = GR;
+    out.q_gs = 0;
+    out.q_smem = 0;
+    if (staged) {
+        std::vector<int> off;
+        int stage_in = 0;
+        for (int c : used) {
+            off.push_back(stage_in);
+            stage_in += ((R * compact_bytes(cols[c].precision) + 16 + 15) / 16) * 16;
+        }
+        const int off_gid = stage_in;
+        stage_in += R * 4 + 16;
+        const int off_acc = 2 * stage_in;
+        const int budget = 48 * 1024 - off_acc - 64;
+        int GS = std::min(4096, budget / (W * 4 + 4));
+        if (GS < GR) GS = GR;
+        const int off_cnt = off_acc + ((GS * W * 4 + 15) / 16) * 16;
+        const int off_bar = off_cnt + ((GS * 4 + 15) / 16) * 16;
+        const int smem = off_bar + 16;
+        out.q_gs = GS;
+        out.q_smem = smem;
+        int tile_in_bytes = R * 4;
+        for (int c : used) tile_in_bytes += R * compact_bytes(cols[c].precision);
+        src << "template <int MODE>\nUP_DI void up_query_tile_body(const UpQArgs& a, u8* sm) {\n";
+        src << "    constexpr int R = " << R << ";\n    constexpr int W = " << W << ";\n";
+        src << "    constexpr int GR = " << std::max(GR, 1) << ";\n";
+        src << "    u64* bar = (u64*)(sm + " << off_bar << ");\n";
+        src << "    u32* sacc = (u32*)(sm + " << off_acc << ");\n";
+        src << "    u32* scnt = (u32*)(sm + " << off_cnt << ");\n";
+        src << "    const int ng = a.n_groups;\n";
+        src << "    const int nsm = MODE == 0 ? (ng < GR ? ng : GR) : (MODE == 1 ? ng : 0);\n";
+        src << "    for (int i = threadIdx.x; i < nsm * W; i += blockDim.x) sacc[i] = 0u;\n";
+        src << "    for (int i = threadIdx.x; i < nsm; i += blockDim.x) scnt[i] = 0u;\n";
+        for (int i = 0; i < NR; i++)
+            src << "    u32 ra" << i << "[MODE == 0 ? GR : 1][" << acc_limbs[i] << "];\n";
+        src << "    u32 rc[MODE == 0 ? GR : 1];\n";
+        src << "#pragma unroll\n    for (int j = 0; j < (MODE == 0 ? GR : 1); j++) {\n        rc[j] = 0u;\n";
+        for (int i = 0; i < NR; i++)
+            src << "#pragma unroll\n        for (int l = 0; l < " << acc_limbs[i] << "; l++) ra" << i << "[j][l] = 0u;\n";
+        src << "    }\n";
+        src << "    const i64 ntiles = (a.rows + R - 1) / R;\n";
+        src << "    const i64 nfull = a.vec_ok ? a.rows / R : 0;  // tiles moved by bulk copies\n";
+        src << "    u32 err = 0u;\n";
+        src << "    if (threadIdx.x == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); mbar_init_fence(); }\n";
+        src << "    __syncthreads();\n";
+        src << "    auto issue = [&](i64 tt, int st) {\n";
+        src << "        mbar_expect_tx(&bar[st], " << tile_in_bytes << "u);\n";
+        for (size_t i = 0; i < used.size(); i++) {
+            int c = used[i];
+            int B = compact_bytes(cols[c].precision);
+            src << "        bulk_load(sm + st * " << stage_in << " + " << off[i] << ", a.col[" << c
+                << "].data + tt * (i64)(R * " << B << "), " << R * B << "u, &bar[st]);\n";
+        }
+        src << "        bulk_load(sm + st * " << stage_in << " + " << off_gid
+            << ", (const u8*)(a.gid + tt * (i64)R), " << R * 4 << "u, &bar[st]);\n";
+        src << "    };\n";
+        src << "    if (threadIdx.x == 0 && (i64)blockIdx.x < nfull) issue(blockIdx.x, 0);\n";
+        src << "    int k = 0;\n";
+        src << "    bool timed_out = false;\n    int to_st = 0;\n    u32 to_par = 0u;\n";
+        src << "    for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {\n";
+        src << "        const int st = k & 1;\n";
+        src << "        const i64 row0 = t * (i64)R;\n";
+        src << "        const int nr = (a.rows - row0) < R ? (int)(a.rows - row0) : R;\n";
+        src << "        const bool bulk = t < nfull;\n";
+        src << "        const i64 tn = t + gridDim.x;\n";
+        src << "        if (threadIdx.x == 0 && tn < nfull) issue(tn, st ^ 1);\n";
+        src << "        u8* in = sm + st * " << stage_in << ";\n";
+        src << "        if (bulk) {\n";
+        src << "            if (!mbar_wait(&bar[st], (u32)((k >> 1) & 1))) { timed_out = true; to_st = st; to_par = (u32)((k >> 1) & 1); }\n";
+        src << "        } else {\n";
+        for (size_t i = 0; i < used.size(); i++) {
+            int c = used[i];
+            int B = compact_bytes(cols[c].precision);
+            src << "            tile_copy_in(in + " << off[i] << ", a.col[" << c << "].data + row0 * " << B << ", nr * "
+                << B << ", a.vec_ok != 0);\n";
+        }
+        src << "            tile_copy_in(in + " << off_gid << ", (const u8*)(a.gid + row0), nr * 4, a.vec_ok != 0);\n";
+        src << "            __syncthreads();\n";
+        src << "        }\n";
+        src << "        if (__syncthreads_or(timed_out)) break;\n";
+        src << "        const int* tg = (const int*)(in + " << off_gid << ");\n";
+        src << "        for (int r = threadIdx.x; r < nr; r += blockDim.x) {\n";
+        src << "            const int g = tg[r];\n";
+        src << "            if ((unsigned)g >= (unsigned)ng) { err |= ERR_DOMAIN; continue; }\n";
+        src << decl_t("            ");
+        if (NR > 0) {
+            src << "            err |= up_qvals(";
+            for (size_t i = 0; i < used.size(); i++)
+                src << "in + " << off[i] << " + r * " << compact_bytes(cols[used[i]].precision) << ", ";
+            src << "true" << targs() << ");\n";
+        }
+        src << "            if constexpr (MODE == 0) {\n";
+        src << "#pragma unroll\n                for (int j = 0; j < GR; j++)\n";
+        src << "                    if (g == j) {\n                        rc[j]++;\n";
+        for (int i = 0; i < NR; i++) src << "                        add_twos(ra" << i << "[j], qv" << i << ");\n";
+        src << "                    }\n";
+        src << "            } else if constexpr (MODE == 1) {\n";
+        src << "                atomicAdd(scnt + g, 1u);\n";
+        for (int i = 0; i < NR; i++)
+            src << "                atomic_add_twos(sacc + g * W + " << acc_off[i] << ", qv" << i << ");\n";
+        src << "            } else {\n";
+        src << "                atomicAdd(a.cnt + g, 1ull);\n";
+        for (int i = 0; i < NR; i++)
+            src << "                atomic_add_twos(a.acc + (i64)g * W + " << acc_off[i] << ", qv" << i << ");\n";
+        src << "            }\n";
+        src << "        }\n";
+        src << "        __syncthreads();\n";
+        src << "    }\n";
+        src << "    if (threadIdx.x == 0 && timed_out) {\n";
+        src << "        err |= ERR_TIMEOUT;\n";
+        src << "        mbar_wait(&bar[to_st], to_par);  // bounded: let copies in flight land before exit\n";
+        src << "    }\n";
+        src << "    if constexpr (MODE == 0) {\n";
+        src << "#pragma unroll\n        for (int j = 0; j < GR; j++)\n";
+        src << "            if (rc[j] != 0u) {\n";
+        src << "                atomicAdd(scnt + j, rc[j]);\n";
+        for (int i = 0; i < NR; i++)
+            src << "                atomic_add_twos(sacc + j * W + " << acc_off[i] << ", ra" << i << "[j]);\n";
+        src << "            }\n";
+        src << "    }\n";
+        src << "    if constexpr (MODE != 2) {\n";
+        src << "        __syncthreads();\n";
+        src << "        for (int gg = threadIdx.x; gg < nsm; gg += blockDim.x) {\n";
+        src << "            const u32 c = scnt[gg];\n";
+        src << "            if (c == 0u) continue;\n";
+        src << "            atomicAdd(a.cnt + gg, (u64)c);\n";
+        for (int i = 0; i < NR; i++) {
+            src << "            {\n                u32 m[" << acc_limbs[i] << "];\n";
+            src << "#pragma unroll\n                for (int l = 0; l < " << acc_limbs[i] << "; l++) m[l] = sacc[gg * W + "
+                << acc_off[i] << " + l];\n";
+            src << "                atomic_add_twos(a.acc + (i64)gg * W + " << acc_off[i] << ", m);\n            }\n";
+        }
+        src << "        }\n";
+        src << "    }\n";
+        src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
+        src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n";
+        src << "}\n\n";
+        const char* names[3] = {"up_query_tile_r", "up_query_tile_s", "up_query_tile_g"};
+        for (int mde = 0; mde < 3; mde++) {
+            if (mde == 0 && GR == 0) continue;
+            src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") " << names[mde]
+                << "(const UpQArgs a) {\n    extern __shared__ __align__(128) u8 sm[];\n    up_query_tile_body<" << mde
+                << ">(a, sm);\n}\n\n";
+        }
+    }
 
     src << "extern \"C\" __global__ void __launch_bounds__(256) up_query_fin(const UpQArgs a) {\n";
     src << "    const int g = blockIdx.x * blockDim.x + threadIdx.x;\n";
@@ -562,6 +749,11 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
 
     out.source = src.str();
     out.kernels = {"up_query_acc", "up_query_fin"};
+    if (out.q_staged) {
+        if (out.q_gr > 0) out.kernels.push_back("up_query_tile_r");
+        out.kernels.push_back("up_query_tile_s");
+        out.kernels.push_back("up_query_tile_g");
+    }
     out.block_threads = T;
     out.in_bytes.assign(n_cols, 0);
     for (int c = 0; c < n_cols; c++) out.in_bytes[c] = compact_bytes(cols[c].precision) + (cols[c].nullable ? 1 : 0);

@@ -599,11 +599,8 @@ UP_DI void tile_copy_out(u8* __restrict__ dst, const u8* __restrict__ src, int n
 // Two's complement accumulation of a sign-magnitude value into NACC limbs in
 // memory with 32-bit atomics, carries propagated limb by limb.  Exact as long
 // as the true sum fits NACC limbs signed (the host sizes NACC for that).
-template <int NACC, int N>
-UP_DI void atomic_acc_add(u32* acc, const u32 (&m)[N], u32 sign) {
-    u32 t[NACC];
-    copy_ext(t, m);
-    if (sign) negate(t);
+template <int NACC>
+UP_DI void atomic_add_twos(u32* acc, const u32 (&t)[NACC]) {
     u32 carry = 0;
 #pragma unroll
     for (int i = 0; i < NACC; i++) {
@@ -616,6 +613,32 @@ UP_DI void atomic_acc_add(u32* acc, const u32 (&m)[N], u32 sign) {
         }
         carry = c1;
     }
+}
+
+// Two's complement image over N limbs of a sign-magnitude value.
+template <int N, int M>
+UP_DI void to_twos(u32 (&t)[N], const u32 (&m)[M], u32 sign) {
+    copy_ext(t, m);
+    if (sign) negate(t);
+}
+
+// r += t modulo 2^(32N) (two's complement accumulate in registers).
+template <int N>
+UP_DI void add_twos(u32 (&r)[N], const u32 (&t)[N]) {
+    u64 c = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        c += (u64)r[i] + t[i];
+        r[i] = (u32)c;
+        c >>= 32;
+    }
+}
+
+template <int NACC, int N>
+UP_DI void atomic_acc_add(u32* acc, const u32 (&m)[N], u32 sign) {
+    u32 t[NACC];
+    to_twos(t, m, sign);
+    atomic_add_twos(acc, t);
 }
 
 // The reference's nullable_type<Decimal> image of a SUM/AVG result

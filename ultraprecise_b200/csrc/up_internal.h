@@ -68,7 +68,12 @@ struct GeneratedModule {
     // query modules
     int n_aggs = 0;
     std::vector<int> agg_kind, agg_scale, agg_acc_limbs, agg_acc_offset;
-    int acc_words_per_group = 0;  // sum over aggregates (count excluded)
+    int acc_words_per_group = 0;  // one accumulator per distinct aggregated expression
+    bool q_staged = false;        // tile kernels (bulk-copy staged inputs) were generated
+    int q_tile_rows = 0;          // rows per tile of the tile kernels
+    int q_gr = 0;                 // up_query_tile_r handles n_groups <= q_gr
+    int q_gs = 0;                 // up_query_tile_s handles n_groups <= q_gs
+    int q_smem = 0;               // dynamic shared memory of the tile kernels
 };
 up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
                                int n_cols, const up_compile_opts* opts, GeneratedModule& out);

@@ -129,12 +129,19 @@ up_status nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::s
     const char* hdr_name[1] = {"up_dev.cuh"};
     nvrtcResult r = nvrtcCreateProgram(&prog, src.c_str(), "up_kernel.cu", 1, hdr_src, hdr_name);
     if (r != NVRTC_SUCCESS) return fail(UP_ERR_COMPILE, std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r));
-    const char* opts[] = {kArch, "-std=c++17", "-lineinfo", "--restrict", "-DUP_NVRTC=1", "-rdc=true"};
-    r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])) - (rdc ? 0 : 1), opts);
+    // UP_JIT_VERBOSE=1 adds ptxas's resource report (registers, spills,
+    // shared memory per kernel) and prints the compile log to stderr.
+    const char* vb = getenv("UP_JIT_VERBOSE");
+    const bool verbose = vb && *vb && *vb != '0';
+    std::vector<const char*> opts = {kArch, "-std=c++17", "-lineinfo", "--restrict", "-DUP_NVRTC=1"};
+    if (rdc) opts.push_back("-rdc=true");
+    if (verbose) opts.push_back("--ptxas-options=-v");
+    r = nvrtcCompileProgram(prog, (int)opts.size(), opts.data());
     size_t ls = 0;
     nvrtcGetProgramLogSize(prog, &ls);
     log.assign(ls, '\0');
     if (ls) nvrtcGetProgramLog(prog, &log[0]);
+    if (verbose) fprintf(stderr, "%s\n", log.c_str());
     if (r != NVRTC_SUCCESS) {
         nvrtcDestroyProgram(&prog);
         return fail(UP_ERR_COMPILE, "NVRTC: " + std::string(nvrtcGetErrorString(r)) + "\n" + log);
@@ -174,7 +181,8 @@ up_status jit_compile_unit(const std::string& src, bool rdc, std::vector<char>& 
     snprintf(name, sizeof name, "%016llx", (unsigned long long)h);
     std::string dir = cache_dir();
     std::string base = dir + "/" + name;
-    if (disk_cache_enabled()) {
+    const char* vb = getenv("UP_JIT_VERBOSE");
+    if (disk_cache_enabled() && !(vb && *vb && *vb != '0')) {
         std::string k2, bin;
         if (read_file(base + ".key", k2) && k2 == key && read_file(base + ".cubin", bin) && !bin.empty()) {
             cubin.assign(bin.begin(), bin.end());
