@@ -147,6 +147,12 @@ def build_expr(case):
     return sweep_expr(case["p"], case["op"])
 
 
+# DRAM bytes per row (dram__bytes_read.sum + dram__bytes_write.sum of one ncu
+# capture, divided by the rows of the captured launch) for the sweep cases
+# profiled so far: profiles/up_expr_tile_p600_mad.md, up_expr_tile_p38_mad.md.
+NCU_TRAFFIC_PER_ROW = {(600, "mad"): 334.6e6 / 262144, (38, "mad"): 301.58e6 / 4194304}
+
+
 # ---------------------------------------------------------- our arm
 def run_ours(args, rank, world):
     import torch
@@ -221,15 +227,20 @@ def run_ours(args, rank, world):
                          "int_gmadds": round(gmadds, 1), "int_frac": round(gmadds * 1e9 / madd_peak.value, 4)})
     dom = max(range(len(cases)), key=lambda i: per_case[i])
     dc, dr = cases[dom], case_rep[dom]
+    tr = NCU_TRAFFIC_PER_ROW.get((dc["p"], dc["op"]))
+    traffic = round(tr * dc["rows"]) if tr else None
     hbm_bound = dr["hbm_frac"] >= dr["int_frac"]
     if hbm_bound:
         roof = {"bound": "hbm", "achieved": dr["hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(dr["hbm_gbs"] / hbm_peak, 4), "traffic": None,
-                "kernel": f"up_expr_tile p={dc['p']} {dc['op']}", "peak_source": peak_kind}
+                "frac": round(dr["hbm_gbs"] / hbm_peak, 4), "traffic": traffic,
+                "kernel": f"up_expr_tile p={dc['p']} {dc['op']}", "peak_source": peak_kind,
+                "algorithmic_bytes": dc["bytes_per_row"] * dc["rows"]}
     else:
         roof = {"bound": "int32", "achieved": dr["int_gmadds"], "peak": round(madd_peak.value / 1e9, 1),
-                "unit": "G limb-madd/s", "frac": dr["int_frac"], "traffic": None,
+                "unit": "G limb-madd/s", "frac": dr["int_frac"], "traffic": traffic,
                 "kernel": f"up_expr_tile p={dc['p']} {dc['op']}",
+                "algorithmic_bytes": dc["bytes_per_row"] * dc["rows"],
+                "madds_per_row": dc["madds_per_row"],
                 "peak_source": "measured (up_util_imad_peak)",
                 "hbm_achieved_gbs": dr["hbm_gbs"], "hbm_frac": dr["hbm_frac"]}
     res = {"metric": METRIC, "value": round(value), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
@@ -548,12 +559,15 @@ def run_query(args, rank, world):
         with torch.cuda.stream(stream):
             cols, k1, k2 = query_inputs(rows, 20261203 + 7 * rank, stream)
             torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            gid, G, _ = runtime.group_ids_from_keys([k1, k2], [1, 1], stream=stream)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            gid_ms = e0.elapsed_time(e1)
+            gid, G, _ = runtime.group_ids_from_keys([k1, k2], [1, 1], stream=stream)  # warm (module load)
+            gid_ms = 1e30
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                gid, G, _ = runtime.group_ids_from_keys([k1, k2], [1, 1], stream=stream)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                gid_ms = min(gid_ms, e0.elapsed_time(e1))
         dc = [runtime.DeviceColumn(c, 15, 2) for c in cols]
         outs = [torch.empty(G * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES), dtype=torch.uint8,
                             device="cuda") for k, _ in aggs]
