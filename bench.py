@@ -1,7 +1,7 @@
 """Benchmark of the exact-decimal path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sweep|batch|query]
+                    [--workload sweep|batch|query|sin|serve]
 
 Workload "sweep" (default) is the precision sweep: element-wise a*b+c and a/b
 (scale s+4, half-up) on DECIMAL(p, p/4), p in {18,38,76,150,300,600}, every
@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query", "sin", "serve"])
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per rate (serve workload)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -691,6 +692,303 @@ def query_cpu_rate(cpu_seconds, threads, seed=3):
     return rows / run(rows), rows
 
 
+# ------------------------------------------------------------ sin workload
+SIN_METRIC = "decimal rows/s (sin(x) 20-term Horner series on DECIMAL(p,p-2), p=100/300/1000), bit-exact"
+
+
+def sin_madds_per_row(p):
+    """Limb multiply-adds per row: per Horner step one L x L product, its
+    truncation by 10^(p-2) (a 2L by ~L long division) and the division by a
+    one-limb integer; plus x*x and the final x*t."""
+    from ultraprecise_b200 import codec, workloads
+    L = (codec.compact_bytes(p) + 3) // 4
+    lp = ((10 ** (p - 2)).bit_length() + 31) // 32
+    step = L * L + (2 * L - lp + 1) * lp + 2 * L
+    return (workloads.SIN_TERMS - 1) * step + 2 * (L * L + (2 * L - lp + 1) * lp)
+
+
+def run_sin(args, rank, world):
+    import torch
+    from ultraprecise_b200 import abi, codec, runtime, workloads
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = abi.load()
+    stream = torch.cuda.Stream()
+    madd_peak = C.c_double(0)
+    abi.check(lib.up_util_imad_peak(C.byref(madd_peak), stream.cuda_stream), "imad peak")
+    hbm_peak, peak_kind = peaks()
+    cases = []
+    for p, rows in workloads.SIN:
+        rows = max(1, int(rows * args.rows_scale))
+        e, cols = workloads.sin_expr(p)
+        m = runtime.compile_expr(e, cols)
+        raw = workloads.sin_inputs(p, rows, seed=20261203 + p + 7 * rank)
+        host = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
+        d = runtime.DeviceColumn(host.cuda(), p, p - 2)
+        out = torch.empty(rows * m.value_bytes, dtype=torch.uint8, device="cuda")
+        cases.append({"p": p, "rows": rows, "mod": m, "in": d, "out": out, "host": host,
+                      "bytes_per_row": 2 * codec.compact_bytes(p), "madds_per_row": sin_madds_per_row(p)})
+    torch.cuda.synchronize()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in cases]
+           for _ in range(args.steps)]
+
+    def launch(c):
+        c["mod"].launch([c["in"]], c["rows"], out=c["out"], err=err, stream=stream)
+
+    for _ in range(args.warmup):
+        for c in cases:
+            launch(c)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        t0.record(stream)
+        for k in range(args.steps):
+            for i, c in enumerate(cases):
+                evs[k][i][0].record(stream)
+                launch(c)
+                evs[k][i][1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    ms = max_over_ranks(t0.elapsed_time(t1), world) / args.steps
+    rows = sum(c["rows"] for c in cases)
+    rep = []
+    for i, c in enumerate(cases):
+        cm = sum(evs[k][i][0].elapsed_time(evs[k][i][1]) for k in range(args.steps)) / args.steps
+        gm = c["madds_per_row"] * c["rows"] / (cm * 1e-3) / 1e9
+        rep.append({"p": c["p"], "rows": c["rows"], "ms": round(cm, 4), "rows_per_s": round(c["rows"] / (cm * 1e-3)),
+                    "int_gmadds": round(gm, 1), "int_frac": round(gm * 1e9 / madd_peak.value, 4),
+                    "madds_per_row": c["madds_per_row"]})
+    dom = max(range(len(rep)), key=lambda i: rep[i]["ms"])
+    res = {"metric": SIN_METRIC, "value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+           "config": {"workload": "sin(x) 20-term Horner on DECIMAL(p,p-2): 1M rows p=100, 512K p=300, "
+                                  "256K p=1000; x uniform in [-pi, pi]", "rows_per_step_per_gpu": rows,
+                      "l2": "compute-bound; inputs stay resident", "parallelism": f"replicas x{world}"},
+           "roofline": {"bound": "int32", "achieved": rep[dom]["int_gmadds"],
+                        "peak": round(madd_peak.value / 1e9, 1), "unit": "G limb-madd/s",
+                        "frac": rep[dom]["int_frac"], "traffic": None,
+                        "kernel": f"up_expr_tile sin p={rep[dom]['p']}",
+                        "peak_source": "measured (up_util_imad_peak)"},
+           "cases": rep, "gpu_launches": len(cases) * args.steps, "clocks": clk.summary()}
+    if not args.no_e2e:
+        h2d = sum(c["host"].numel() for c in cases)
+        hout = [torch.empty(c["out"].numel(), dtype=torch.uint8, pin_memory=True) for c in cases]
+        pins = [c["host"].pin_memory() for c in cases]
+        d2h = sum(h.numel() for h in hout)
+
+        def e2e_step():
+            with torch.cuda.stream(stream):
+                for c, hp, ho in zip(cases, pins, hout):
+                    c["in"].data.copy_(hp, non_blocking=True)
+                    launch(c)
+                    ho.copy_(c["out"], non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        n = max(1, min(args.steps, 3))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1), world) / n
+        res["e2e"] = {"value": round(rows * world / (ems * 1e-3)), "unit": "rows/s", "h2d_bytes_per_step": h2d,
+                      "d2h_bytes_per_step": d2h, "ms_per_step": round(ems, 3), "steps": n}
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        rate, sample = sin_cpu_rate(args.cpu_seconds, os.cpu_count() or 1)
+        res["cpu_baseline"] = {"value": round(rate), "unit": "rows/s", "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": sample}
+    return res
+
+
+def sin_cpu_rate(cpu_seconds, threads, seed=11):
+    """Oracle rows/s over the same three-precision mix, every case at one
+    common fraction of its rows, sized for ~cpu_seconds."""
+    from oracle import oracle
+    from ultraprecise_b200 import codec, workloads
+    from ultraprecise_b200 import expr as E
+    built = []
+    for p, rows in workloads.SIN:
+        e, cols = workloads.sin_expr(p)
+        b = E.build([e], cols)
+        E.derive_types(b)
+        built.append((p, rows, b))
+
+    def run(frac):
+        secs, tot = 0.0, 0
+        for p, rows, b in built:
+            r = max(8, int(rows * frac))
+            raw = workloads.sin_inputs(p, r, seed + p)
+            t = time.perf_counter()
+            oracle.eval_expr(b, b.roots[0], [raw], r, codec.compact_bytes(p), threads=threads)
+            secs += time.perf_counter() - t
+            tot += r
+        return tot, secs
+
+    r0, s0 = run(1.0 / 2048)
+    frac = min(1.0 / 8, (1.0 / 2048) * cpu_seconds / max(s0, 1e-4))
+    r1, s1 = run(frac)
+    return r1 / s1, f"{r1} rows: every case at {frac:.2e} of its rows (same mix), oracle on {threads} host threads"
+
+
+# ------------------------------------------------------------ serve workload
+SERVE_METRIC = "served queries/s and p50/p95/p99 latency (open-loop Poisson, mixed decimal queries), bit-exact"
+
+
+def serve_shapes(rank):
+    """Resident columns and modules of every request shape, per kind."""
+    import torch
+    from ultraprecise_b200 import runtime, workloads
+    kinds = [[], [], [], []]
+    exprs, aggs, ct = workloads.query_exprs()
+    q = runtime.compile_query(exprs, aggs, ct)
+    rows = (1 << 20) // 10
+    cols, k1, k2 = query_inputs(rows, 77 + rank)
+    gid, G, _ = runtime.group_ids_from_keys([k1, k2], [1, 1])
+    kinds[0].append({"mod": q, "cols": [runtime.DeviceColumn(c, 15, 2) for c in cols], "rows": rows, "gid": gid,
+                     "G": G, "name": "query"})
+    for p, r in workloads.SWEEP:
+        for op in workloads.SWEEP_OPS:
+            e, ctp = workloads.sweep_expr(p, op)
+            rr = max(1, r // 10)
+            dc = [runtime.DeviceColumn(runtime.gen_digits(rr, p, 1000 + p + k, nonzero=(op == "div" and k == 1)),
+                                       p, p // 4) for k in range(len(ctp))]
+            kinds[1].append({"mod": runtime.compile_expr(e, ctp), "cols": dc, "rows": rr, "gid": None, "G": 0,
+                             "name": f"sweep p={p} {op}"})
+    tasks, _ = workloads.batch_tasks(row_scale=0.1)
+    data = workloads.batch_columns(tasks, seed=9)
+    for k, (t, (rr, cl, g)) in enumerate(zip(tasks, data)):
+        dc = [runtime.DeviceColumn(c, t["p"], t["s"]) for c in cl]
+        if t["agg"] < 0:
+            kinds[2].append({"mod": runtime.compile_expr(t["expr"], t["cols"]), "cols": dc, "rows": rr, "gid": None,
+                             "G": 0, "name": f"task {k}"})
+        else:
+            kinds[2].append({"mod": runtime.compile_query([t["expr"]], [(t["agg"], 0)], t["cols"]), "cols": dc,
+                             "rows": rr, "gid": torch.from_numpy(g).cuda(), "G": t["groups"], "name": f"task {k}"})
+    for p, r in workloads.SIN:
+        e, ctp = workloads.sin_expr(p)
+        rr = max(1, r // 10)
+        raw = workloads.sin_inputs(p, rr, 300 + p)
+        dc = [runtime.DeviceColumn(torch.frombuffer(bytearray(raw), dtype=torch.uint8).cuda(), p, p - 2)]
+        kinds[3].append({"mod": runtime.compile_expr(e, ctp), "cols": dc, "rows": rr, "gid": None, "G": 0,
+                         "name": f"sin p={p}"})
+    return kinds
+
+
+def run_serve(args, rank, world):
+    import collections
+    import random
+    import torch
+    from ultraprecise_b200 import serve, workloads
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    kinds = serve_shapes(rank)
+    n_parts = lambda s: len(s["mod"].aggs) if s["gid"] is not None else 1
+    # each shape alone through the plain path: reference bytes
+    for kl in kinds:
+        for s in kl:
+            if s["gid"] is None:
+                s["alone"] = [s["mod"].launch(s["cols"], s["rows"]).clone()]
+            else:
+                s["alone"] = [o.clone() for o in s["mod"].launch(s["cols"], s["gid"], s["G"])]
+    torch.cuda.synchronize()
+
+    def trace(rate):
+        arr = workloads.poisson_arrivals(rate, args.serve_seconds, seed=int(rate) + rank)
+        kk = workloads.serve_kinds(len(arr), seed=int(rate) * 7 + rank)
+        rng = random.Random(int(rate) * 13 + rank)
+        return [(t, kinds[k][rng.randrange(len(kinds[k]))]) for t, k in zip(arr, kk)]
+
+    def run_session(tr):
+        sess = serve.Session(n_streams=8)
+        t0 = sess.clock_ms()
+        pending = collections.deque()
+        lat, mismatches, checked = [], 0, 0
+
+        def reap(block):
+            nonlocal mismatches, checked
+            while pending:
+                rid, s, idx = pending[0]
+                st = sess.wait(rid, -1.0) if block else sess.poll(rid)[0]
+                if st not in (serve.DONE, serve.FAILED):
+                    return
+                pending.popleft()
+                stt, l = sess.poll(rid)
+                if stt != serve.DONE:
+                    raise RuntimeError(f"request {rid} failed")
+                lat.append(l)
+                if idx % 16 == 0:  # sampled byte-equality against the query run alone
+                    checked += 1
+                    for part in range(n_parts(s)):
+                        out, _ = sess.result(rid, part)
+                        if not torch.equal(out, s["alone"][part]):
+                            mismatches += 1
+                sess.release(rid)
+
+        for i, (t, s) in enumerate(tr):
+            while sess.clock_ms() - t0 < t:
+                reap(False)
+            rid = sess.submit(s["mod"], s["cols"], s["rows"], s["gid"], s["G"], arrival_ms=t0 + t)
+            pending.append((rid, s, i))
+            reap(False)
+        reap(True)
+        end = sess.clock_ms() - t0
+        st = sess.stats()
+        sess.close()
+        p50, p95, p99 = serve.percentiles(lat)
+        return {"queries": len(tr), "seconds": round(end / 1e3, 3), "queries_per_s": round(len(tr) / (end / 1e3), 1),
+                "p50_ms": round(p50, 3), "p95_ms": round(p95, 3), "p99_ms": round(p99, 3),
+                "max_inflight": st["max_inflight_seen"], "deferred": st["deferred"],
+                "max_outstanding_gb": round(st["max_outstanding_bytes"] / 1e9, 3),
+                "sampled_byte_equal": mismatches == 0, "sampled": checked}
+
+    def run_plain(tr):
+        """The same trace, one query at a time through the plain launch path."""
+        stream = torch.cuda.current_stream()
+        t0 = time.perf_counter() * 1e3
+        lat = []
+        for t, s in tr:
+            now = time.perf_counter() * 1e3 - t0
+            if now < t:
+                time.sleep((t - now) / 1e3)
+            if s["gid"] is None:
+                s["mod"].launch(s["cols"], s["rows"], stream=stream)
+            else:
+                s["mod"].launch(s["cols"], s["gid"], s["G"], stream=stream)
+            stream.synchronize()
+            lat.append(time.perf_counter() * 1e3 - t0 - t)
+        end = time.perf_counter() * 1e3 - t0
+        p50, p95, p99 = serve.percentiles(lat)
+        return {"queries_per_s": round(len(tr) / (end / 1e3), 1), "p50_ms": round(p50, 3),
+                "p95_ms": round(p95, 3), "p99_ms": round(p99, 3), "seconds": round(end / 1e3, 3)}
+
+    warm = trace(200.0)[:50]
+    run_session(warm)
+    run_plain(warm)
+    rates = {}
+    with ClockSampler(dev) as clk:
+        for rate in workloads.SERVE_RATES:
+            tr = trace(float(rate))
+            rates[str(rate)] = {"served": run_session(tr), "plain": run_plain(tr)}
+    top = rates[str(workloads.SERVE_RATES[-1])]
+    # value: the highest offered rate's served throughput
+    res = {"metric": SERVE_METRIC, "value": top["served"]["queries_per_s"], "unit": "queries/s", "n_gpus": world,
+           "steps": len(workloads.SERVE_RATES), "warmup": 1, "ms_per_step": round(top["served"]["seconds"] * 1e3, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+           "config": {"workload": f"open-loop Poisson at {list(workloads.SERVE_RATES)} q/s, "
+                                  f"{args.serve_seconds} s of arrivals each; mix 40/30/20/10 of query/sweep/"
+                                  f"batch-task/sin shapes at 1/10 rows; resident columns",
+                      "parallelism": f"replicas x{world}", "streams": 8},
+           "rates": rates, "gpu_launches": None, "clocks": clk.summary()}
+    res["roofline"] = None
+    return res
+
+
 # ------------------------------------------------------ CPU baseline
 def cpu_rate(cases, cpu_seconds, threads, seed=1):
     """Time the oracle on the host cores over the same sweep mix (every case
@@ -737,6 +1035,26 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
+    if args.workload == "serve":
+        return {"impl": "reference", "unavailable": "the reference has no serving loop; its CPU decimal path is "
+                                                    "timed by the other workloads"}
+    if args.workload == "sin":
+        per = args.cpu_seconds / max(1, args.steps)
+        rates, sample = [], ""
+        for k in range(max(1, args.steps)):
+            r, sample = sin_cpu_rate(per, threads, seed=11 + k)
+            rates.append(r)
+        rate = sorted(rates)[len(rates) // 2]
+        from ultraprecise_b200 import workloads
+        total = sum(r for _, r in workloads.SIN)
+        return {"metric": SIN_METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(total / rate * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+                "impl": "reference", "config": {"workload": "sin series on host cores, bounded sample",
+                                                "parallelism": f"{threads} host threads"},
+                "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "query":
         per = args.cpu_seconds / max(1, args.steps)
         rates, rows = [], 0
@@ -823,7 +1141,7 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    run = {"batch": run_batch, "query": run_query}.get(args.workload, run_ours)
+    run = {"batch": run_batch, "query": run_query, "sin": run_sin, "serve": run_serve}.get(args.workload, run_ours)
     res = run(args, rank, world)
     if world > 1:
         import torch.distributed as dist

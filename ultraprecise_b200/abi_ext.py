@@ -21,4 +21,14 @@ SIGNATURES = {
     "up_batch_task_type": (_I32, [_P, _I32, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32)]),
     "up_batch_release": (None, [_P]),
     "up_util_compile_batch_only": (_I32, [_P, _I32]),
+    # ultraprecise_serve.h
+    "up_serve_create": (_I32, [_P, C.POINTER(_P)]),
+    "up_serve_clock_ms": (C.c_double, [_P]),
+    "up_serve_submit": (_I32, [_P, _P, C.POINTER(_I64)]),
+    "up_serve_poll": (_I32, [_P, _I64, C.POINTER(_I32), C.POINTER(C.c_double)]),
+    "up_serve_wait": (_I32, [_P, _I64, C.c_double, C.POINTER(_I32)]),
+    "up_serve_result": (_I32, [_P, _I64, _I32, C.POINTER(_P), C.POINTER(_I64), C.POINTER(C.c_uint32)]),
+    "up_serve_release": (_I32, [_P, _I64]),
+    "up_serve_stats_get": (_I32, [_P, _I32, _P]),
+    "up_serve_destroy": (None, [_P]),
 }

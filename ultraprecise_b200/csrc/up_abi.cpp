@@ -197,6 +197,13 @@ int32_t up_module_cache_size(int32_t clear) { return jit_cache_size(clear != 0);
 
 up_status up_expr_launch(up_module* m, const up_column* in, int32_t n_in, int64_t rows, void* out,
                          uint32_t* err_word, void* stream) {
+    return expr_launch_ex(m, in, n_in, rows, out, err_word, stream, false);
+}
+
+}  // extern "C"
+
+up_status expr_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, void* out,
+                         uint32_t* err_word, void* stream, bool spread) {
     if (!m || m->is_query) return fail(UP_ERR_INVALID_ARG, "not an expression module");
     if (rows < 0) return fail(UP_ERR_INVALID_ARG, "negative row count");
     if (rows == 0) return UP_OK;
@@ -223,18 +230,21 @@ up_status up_expr_launch(up_module* m, const up_column* in, int32_t n_in, int64_
         st = set_smem(k, g.smem_bytes);
         if (st != UP_OK) return st;
         const int64_t ntiles = (rows + g.tile_rows - 1) / g.tile_rows;
-        const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, g.smem_bytes);
+        const int64_t cap = spread ? (int64_t)INT32_MAX : (int64_t)sms * occupancy(k, g.block_threads, g.smem_bytes);
         const unsigned grid = (unsigned)std::min<int64_t>(ntiles, cap);
         UP_CUDA(cudaLaunchKernel((const void*)k, dim3(grid), dim3(g.block_threads), args, (size_t)g.smem_bytes, s));
     } else {
         void* k = jit_kernel(*m->jm.ks, "up_expr_generic");
         const int64_t blocks = (rows + g.block_threads - 1) / g.block_threads;
-        const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, 0) * 4;
+        const int64_t cap = spread ? (int64_t)INT32_MAX : (int64_t)sms * occupancy(k, g.block_threads, 0) * 4;
         const unsigned grid = (unsigned)std::min<int64_t>(blocks, cap);
         UP_CUDA(cudaLaunchKernel((const void*)k, dim3(grid), dim3(g.block_threads), args, 0, s));
     }
     return UP_OK;
 }
+
+extern "C" {
+
 
 up_status up_query_compile(const up_expr_node* nodes, int32_t n_nodes, const up_col_type* cols, int32_t n_cols,
                            const up_query_agg* aggs, int32_t n_aggs, const up_compile_opts* opts, up_module** out) {
@@ -256,6 +266,13 @@ up_status up_query_compile(const up_expr_node* nodes, int32_t n_nodes, const up_
 
 up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
                           int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream) {
+    return query_launch_ex(m, in, n_in, rows, group_ids, n_groups, outs, err_word, stream, false);
+}
+
+}  // extern "C"
+
+up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
+                          int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread) {
     if (!m || !m->is_query) return fail(UP_ERR_INVALID_ARG, "not a query module");
     if (rows < 0 || n_groups < 0) return fail(UP_ERR_INVALID_ARG, "negative size");
     if (n_groups == 0) return UP_OK;
@@ -299,7 +316,9 @@ up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64
             a.vec_ok = (vec_ok && aligned16(group_ids)) ? 1 : 0;
             void* k = jit_kernel(*m->jm.ks, name);
             const int64_t ntiles = (rows + g.q_tile_rows - 1) / g.q_tile_rows;
-            const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, g.q_smem);
+            // the register and shared-memory modes merge once per CTA, so a
+            // spread launch keeps a bounded grid of several waves
+            const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, g.q_smem) * (spread ? 8 : 1);
             e = cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(ntiles, cap)), dim3(g.block_threads),
                                  args, (size_t)g.q_smem, s);
         } else {
@@ -319,6 +338,9 @@ up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64
     if (e2 != cudaSuccess) return cuda_fail(e2, "cudaFreeAsync");
     return UP_OK;
 }
+
+extern "C" {
+
 
 up_status up_group_agg(const up_column* vals, const int32_t* kinds, int32_t n_vals, const int32_t* group_ids,
                        int32_t n_groups, int64_t rows, void* const* outs, uint32_t* err_word, void* stream) {

@@ -43,9 +43,37 @@ struct Emitter {
     std::ostringstream body;
     std::set<int> p10;
     int tmp = 0;
+    bool out_of_line = false;  // call wide operations out of line (see wide_work)
 
     Emitter(const up_expr_node* n, const up_col_type* c, const std::vector<NodeFacts>& facts)
         : nodes(n), cols(c), f(facts) {}
+
+    // Sum of limb-product sizes over the expression's wide operations; above
+    // kOutOfLineWork the operations with at least kWideOp limb products are
+    // called out of line.
+    static constexpr long kOutOfLineWork = 16384;
+    static constexpr long kWideOp = 256;
+    long work = 0;  // limb-product work per row (a cost estimate)
+    void plan(const std::vector<int>& topo) {
+        work = 0;
+        for (int k : topo) work += op_size(k);
+        out_of_line = work > kOutOfLineWork;
+    }
+    long op_size(int k) const {
+        const up_expr_node& nd = nodes[k];
+        switch (nd.kind) {
+            case UP_NODE_MUL: return (long)f[nd.left].limbs * f[nd.right].limbs;
+            case UP_NODE_DIV: return (long)f[k].limbs * f[nd.right].limbs + (long)f[nd.left].limbs * 4;
+            case UP_NODE_RESCALE:
+                return nd.scale < f[nd.left].scale
+                           ? (long)f[nd.left].limbs * limbs_for_bits(big_bitlen(big_pow10(f[nd.left].scale - nd.scale)))
+                           : (long)f[k].limbs;
+            case UP_NODE_ADD:
+            case UP_NODE_SUB: return (long)f[k].limbs * 4;
+            default: return 0;
+        }
+    }
+    const char* sfx(long size) const { return (out_of_line && size >= kWideOp) ? "_ni" : ""; }
 
     std::string p10_name(int k) {
         p10.insert(k);
@@ -65,7 +93,8 @@ struct Emitter {
         std::string t = "t" + std::to_string(tmp++);
         body << "    u32 " << t << "[" << L << "];\n";
         if (p.m.size() == 1) body << "    mul_u32(" << t << ", " << v(a) << ", " << hex32(p.m[0]) << ");\n";
-        else body << "    mul(" << t << ", " << v(a) << ", " << p10_name(d) << ");\n";
+        else body << "    mul" << sfx((long)fa.limbs * (long)p.m.size()) << "(" << t << ", " << v(a) << ", "
+                  << p10_name(d) << ");\n";
         return t;
     }
 
@@ -109,7 +138,8 @@ struct Emitter {
                 break;
             }
             case UP_NODE_MUL:
-                body << "    u32 " << v(k) << "[" << L << "]; mul(" << v(k) << ", " << v(nd.left) << ", "
+                body << "    u32 " << v(k) << "[" << L << "]; mul" << sfx(op_size(k)) << "(" << v(k) << ", "
+                     << v(nd.left) << ", "
                      << v(nd.right) << "); u32 " << s(k) << " = " << s(nd.left) << " ^ " << s(nd.right) << ";\n";
                 break;
             case UP_NODE_DIV: {
@@ -119,7 +149,7 @@ struct Emitter {
                 char w[40];
                 snprintf(w, sizeof w, "0x%016llxull", (unsigned long long)big_low64(p));
                 body << "    u32 " << v(k) << "[" << L << "]; u32 " << s(k) << ";\n";
-                body << "    err |= div_round<" << L << ", " << f[nd.left].limbs << ", " << f[nd.right].limbs << ", "
+                body << "    err |= div_round" << sfx(op_size(k)) << "<" << L << ", " << f[nd.left].limbs << ", " << f[nd.right].limbs << ", "
                      << np << ", " << sh << "u, " << w << ">(" << v(k) << ", " << s(k) << ", " << v(nd.left)
                      << ", " << s(nd.left) << ", " << v(nd.right) << ", " << s(nd.right) << ", " << p10_name(sh)
                      << ");\n";
@@ -137,7 +167,8 @@ struct Emitter {
                     std::string A = aligned(nd.left, nd.scale);
                     body << "    copy_ext(" << v(k) << ", " << A << ");\n";
                 } else {
-                    body << "    trunc_div_pow10(" << v(k) << ", " << v(nd.left) << ", " << p10_name(sa - nd.scale)
+                    body << "    trunc_div_pow10" << sfx(op_size(k)) << "(" << v(k) << ", " << v(nd.left) << ", "
+                         << p10_name(sa - nd.scale)
                          << ");\n";
                 }
                 break;
@@ -229,6 +260,7 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     std::sort(used.begin(), used.end());
 
     Emitter em(nodes, cols, f);
+    em.plan(topo);
     for (int k : topo) em.node(k);
 
     int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
@@ -416,6 +448,7 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
 
     out.source = src.str();
     out.kernels = {"up_expr_tile", "up_expr_generic"};
+    out.work_per_row = em.work + row_bytes;
     out.out_precision = out_p;
     out.out_scale = out_s;
     out.out_bytes = OB;
@@ -499,6 +532,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     const int NR = (int)acc_root.size();
 
     Emitter em(nodes, cols, f);
+    em.plan(topo);
     for (int k : topo) em.node(k);
 
     const int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
@@ -748,6 +782,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     src << "}\n";
 
     out.source = src.str();
+    out.work_per_row = em.work + row_bytes;
     out.kernels = {"up_query_acc", "up_query_fin"};
     if (out.q_staged) {
         if (out.q_gr > 0) out.kernels.push_back("up_query_tile_r");
@@ -827,6 +862,7 @@ up_status generate_batch_module(const BatchTaskDesc* tasks, int n_tasks, Generat
         gt.in_bytes.assign(t.n_cols, 0);
         for (int c = 0; c < t.n_cols; c++) gt.in_bytes[c] = compact_bytes(t.cols[c].precision);
         Emitter em(t.nodes, t.cols, f);
+        em.plan(topo);
         for (int n : topo) em.node(n);
         std::ostringstream src;
         src << kBatchPrelude;

@@ -432,6 +432,27 @@ UP_DI void trunc_div_pow10(u32 (&r)[NR], const u32 (&a)[NA], const u32 (&p10)[NP
     copy_ext(r, q);
 }
 
+// Out-of-line instances of the wide operations.  A module whose expression
+// repeats many wide operations (long series, deep trees of 1000-digit values)
+// calls one instance per operand shape instead of inlining every use: the
+// limb arrays of such widths live in local memory either way, and compile
+// time stays proportional to the number of distinct shapes.
+template <int N, int NA, int NB>
+__device__ __noinline__ void mul_ni(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
+    mul(r, a, b);
+}
+
+template <int NR, int NA, int NB, int NP, u32 SHIFT, u64 P10W>
+__device__ __noinline__ u32 div_round_ni(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32 (&b)[NB],
+                                         u32 sb, const u32 (&p10)[NP]) {
+    return div_round<NR, NA, NB, NP, SHIFT, P10W>(r, sr, a, sa, b, sb, p10);
+}
+
+template <int NR, int NA, int NP>
+__device__ __noinline__ void trunc_div_pow10_ni(u32 (&r)[NR], const u32 (&a)[NA], const u32 (&p10)[NP]) {
+    trunc_div_pow10(r, a, p10);
+}
+
 // Comparison with the reference rules: different signs decide by sign
 // alone (-0 < +0), else aligned magnitudes reversed for negatives.
 // op: 0 <, 1 <=, 2 >, 3 >=, 4 ==, 5 !=

@@ -350,7 +350,13 @@ up_status analyze_nodes(const up_expr_node* nodes, int n_nodes, const up_col_typ
                     if (nd.scale < 0 || nd.scale > kMaxPrecision)
                         return fail(UP_ERR_INVALID_ARG, "rescale target out of range");
                     f.scale = nd.scale;
-                    f.bits = a.bits + (nd.scale > a.scale ? big_bitlen(big_pow10(nd.scale - a.scale)) : 0);
+                    if (nd.scale >= a.scale) {
+                        f.bits = a.bits + (nd.scale > a.scale ? big_bitlen(big_pow10(nd.scale - a.scale)) : 0);
+                    } else {
+                        // |v| < 2^b and 10^d >= 2^(bitlen(10^d)-1), so the
+                        // truncated quotient is below 2^(b - bitlen(10^d) + 1)
+                        f.bits = std::max(1, a.bits - big_bitlen(big_pow10(a.scale - nd.scale)) + 1);
+                    }
                     break;
                 }
                 default:

@@ -74,6 +74,7 @@ struct GeneratedModule {
     int q_gr = 0;                 // up_query_tile_r handles n_groups <= q_gr
     int q_gs = 0;                 // up_query_tile_s handles n_groups <= q_gs
     int q_smem = 0;               // dynamic shared memory of the tile kernels
+    long work_per_row = 0;        // limb-product work + bytes per row (scheduling cost estimate)
 };
 up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
                                int n_cols, const up_compile_opts* opts, GeneratedModule& out);
@@ -132,5 +133,13 @@ struct up_module {
     upi::JitModule jm;
     bool is_query = false;
 };
+
+// Launch variants used by the serving loop: `spread` launches one CTA per
+// tile instead of a persistent grid, so that a long request's CTAs retire
+// often and higher-priority streams get SMs between them.
+up_status expr_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, void* out,
+                         uint32_t* err_word, void* stream, bool spread);
+up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
+                          int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread);
 
 #endif  // UP_INTERNAL_H_

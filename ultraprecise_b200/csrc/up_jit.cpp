@@ -123,6 +123,26 @@ void write_file_atomic(const std::string& p, const std::string& data) {
     rename(tmp.c_str(), p.c_str());
 }
 
+// Look up entry `name` (a .key file holding the full key beside a .cubin)
+// in the cache directory; on a miss, in UP_JIT_CACHE_SEED_DIR, copying a hit
+// into the cache directory (used to rebuild a cache with only the entries a
+// set of compiles still uses).
+bool cache_lookup(const std::string& name, const std::string& key, std::string& bin) {
+    const std::string base = cache_dir() + "/" + name;
+    std::string k2;
+    if (read_file(base + ".key", k2) && k2 == key && read_file(base + ".cubin", bin) && !bin.empty()) return true;
+    const char* seed = getenv("UP_JIT_CACHE_SEED_DIR");
+    if (!seed || !*seed) return false;
+    const std::string sb = std::string(seed) + "/" + name;
+    if (read_file(sb + ".key", k2) && k2 == key && read_file(sb + ".cubin", bin) && !bin.empty()) {
+        mkdirs(cache_dir());
+        write_file_atomic(base + ".cubin", bin);
+        write_file_atomic(base + ".key", key);
+        return true;
+    }
+    return false;
+}
+
 up_status nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::string& log, bool rdc) {
     nvrtcProgram prog;
     const char* hdr_src[1] = {device_header_source().c_str()};
@@ -183,8 +203,8 @@ up_status jit_compile_unit(const std::string& src, bool rdc, std::vector<char>& 
     std::string base = dir + "/" + name;
     const char* vb = getenv("UP_JIT_VERBOSE");
     if (disk_cache_enabled() && !(vb && *vb && *vb != '0')) {
-        std::string k2, bin;
-        if (read_file(base + ".key", k2) && k2 == key && read_file(base + ".cubin", bin) && !bin.empty()) {
+        std::string bin;
+        if (cache_lookup(name, key, bin)) {
             cubin.assign(bin.begin(), bin.end());
             return UP_OK;
         }
@@ -265,8 +285,8 @@ up_status jit_compile_linked(const std::vector<std::string>& units, std::vector<
     const char* vb = getenv("UP_JIT_LINK_VERBOSE");
     const bool verbose = vb && *vb && *vb != '0';
     if (disk_cache_enabled() && !verbose) {
-        std::string k2, bin;
-        if (read_file(base + ".key", k2) && k2 == key && read_file(base + ".cubin", bin) && !bin.empty()) {
+        std::string bin;
+        if (cache_lookup(name, key, bin)) {
             linked.assign(bin.begin(), bin.end());
             return UP_OK;
         }

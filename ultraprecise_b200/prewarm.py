@@ -37,6 +37,9 @@ def prewarm(verbose: bool = False) -> None:
             jobs.append((f"sweep p={p} {op}", [e], cols, None))
     exprs, aggs, cols = workloads.query_exprs()
     jobs.append(("query", exprs, cols, aggs))
+    for p, _ in workloads.SIN:
+        e, cols = workloads.sin_expr(p)
+        jobs.insert(0, (f"sin p={p}", [e], cols, None))  # the longest compiles first
     tasks, _ = workloads.batch_tasks()
     # the plain per-task modules the batched mode is compared against
     for k, t in enumerate(tasks):
@@ -54,5 +57,27 @@ def prewarm(verbose: bool = False) -> None:
         print("prewarmed batch module,", len(tasks), "tasks")
 
 
+def prune(verbose: bool = False) -> None:
+    """Rebuild the in-tree cache with only the entries prewarm() uses: the old
+    cache seeds a fresh directory, which then replaces it."""
+    import os
+    import shutil
+    import subprocess
+    import sys
+    from . import build as B
+    cache = os.path.join(os.path.dirname(os.path.abspath(B.__file__)), "_jitcache")
+    fresh = cache + ".fresh"
+    shutil.rmtree(fresh, ignore_errors=True)
+    env = dict(os.environ, UP_JIT_CACHE_DIR=fresh, UP_JIT_CACHE_SEED_DIR=cache)
+    subprocess.run([sys.executable, "-m", "ultraprecise_b200.prewarm"] + (["-v"] if verbose else []), env=env,
+                   check=True)
+    shutil.rmtree(cache)
+    os.rename(fresh, cache)
+
+
 if __name__ == "__main__":
-    prewarm(verbose=True)
+    import sys
+    if "--prune" in sys.argv:
+        prune(verbose="-v" in sys.argv)
+    else:
+        prewarm(verbose=True)

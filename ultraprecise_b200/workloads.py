@@ -162,3 +162,119 @@ def expr_madds(e, s: int, nbytes: int):
         m += la * lp + max(1, la + lp - lb + 1) * lb
     bits, sc = _bits_bound(e, s, nbytes)
     return m, bits, sc
+
+
+# sin(x) series: 20 terms in Horner form on DECIMAL(p, p-2), x uniform in
+# [-pi, pi] at full scale.  t_20 = 1; t_k = 1 - trunc(y * t_(k+1)) / (2k(2k+1))
+# for k = 19..1 with y = trunc(x*x); sin x = trunc(x * t_1).  Every product and
+# quotient is truncated toward zero to scale p-2 (RESCALE); the divisions by the
+# exact integers 2k(2k+1) (ratios of consecutive factorials) follow the
+# reference's divide rule (scale +4, half-up) before that truncation.
+SIN = [(100, 1 << 20), (300, 1 << 19), (1000, 1 << 18)]
+SIN_TERMS = 20
+
+
+def sin_expr(p: int, terms: int = SIN_TERMS):
+    s = p - 2
+    x = E.col(0)
+    y = E.rescale(x * x, p, s)
+    t = E.dec(10 ** s, scale=s, precision=p)   # 1 at scale p-2
+    one = t
+    for k in range(terms - 1, 0, -1):
+        m = E.rescale(y * t, p, s)
+        d = E.rescale(m / E.lit(2 * k * (2 * k + 1)), p, s)
+        t = E.rescale(one - d, p, s)
+    return E.rescale(x * t, p, s), [E.ColType(p, s)]
+
+
+def pi_scaled(s: int) -> int:
+    """floor(pi * 10^s) by Machin's formula in integer arithmetic."""
+    guard = 10
+    unity = 10 ** (s + guard)
+
+    def arctan_inv(n: int) -> int:
+        total, term, k, sign = 0, unity // n, 1, 1
+        n2 = n * n
+        while term:
+            total += sign * (term // k)
+            term //= n2
+            k += 2
+            sign = -sign
+        return total
+
+    return (4 * (4 * arctan_inv(5) - arctan_inv(239))) // 10 ** guard
+
+
+def sin_inputs(p: int, rows: int, seed: int) -> bytes:
+    """Compact DECIMAL(p, p-2) column of x uniform over [-pi, pi] at full
+    scale: magnitude floor(U * floor(pi * 10^(p-2))) with U uniform on [0,1)
+    drawn to 64 bits beyond the magnitude's width, sign +/- with equal odds."""
+    import random
+    from . import codec
+    rng = random.Random(seed)
+    pi = pi_scaled(p - 2)
+    nb = pi.bit_length() + 64
+    vals = [(rng.getrandbits(1), (rng.getrandbits(nb) * pi) >> nb) for _ in range(rows)]
+    return codec.encode(vals, p)
+
+
+def sin_python(sign: int, mag: int, p: int, terms: int = SIN_TERMS):
+    """The same series in exact Python integers with the decimal path's rules
+    (sign-magnitude values; products and quotients truncated toward zero to
+    scale p-2; division by the integer 2k(2k+1) at scale +4 rounded half up on
+    the magnitude, then truncated): an independent restatement that checks the
+    oracle.  Returns (sign, magnitude) with the sign of zero as computed."""
+    s = p - 2
+    S = 10 ** s
+
+    def mul_trunc(a, b):  # (sign, mag) * (sign, mag), truncated to scale s
+        return (a[0] ^ b[0], (a[1] * b[1]) // S)
+
+    def sub(a, b):  # a - b in sign-magnitude (equal magnitudes give +0)
+        av = -a[1] if a[0] else a[1]
+        bv = -b[1] if b[0] else b[1]
+        v = av - bv
+        return (1 if v < 0 else 0, abs(v))
+
+    x = (sign, mag)
+    y = mul_trunc(x, x)
+    one = (0, S)
+    t = one
+    for k in range(terms - 1, 0, -1):
+        m = mul_trunc(y, t)
+        D = 2 * k * (2 * k + 1)
+        if m[1] == 0:
+            d = (0, 0)  # dividend 0 gives +0
+        else:
+            q, r = divmod(m[1] * 10 ** 4, D)
+            q += 1 if 2 * r >= D else 0
+            d = (m[0], q // 10 ** 4)
+        t = sub(one, d)
+    return mul_trunc(x, t)
+
+
+# Served stream: open-loop Poisson arrivals; each query is drawn 40/30/20/10
+# from the grouped query, the precision-sweep expressions, the batched-set
+# tasks and the sin series, all at 1/10 of their row counts, over columns
+# kept resident in HBM.
+SERVE_RATES = (100, 500, 2000, 5000)
+SERVE_MIX = (0.4, 0.3, 0.2, 0.1)
+
+
+def poisson_arrivals(rate: float, seconds: float, seed: int):
+    """Arrival times in ms of an open-loop Poisson stream (exponential gaps)."""
+    import random
+    rng = random.Random(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.expovariate(rate) * 1000.0
+        if t >= seconds * 1000.0:
+            return out
+        out.append(t)
+
+
+def serve_kinds(n: int, seed: int, mix=SERVE_MIX):
+    """Request kind (0 query, 1 sweep, 2 batch task, 3 sin) per arrival."""
+    import random
+    rng = random.Random(seed)
+    return [rng.choices(range(len(mix)), weights=mix)[0] for _ in range(n)]
