@@ -903,8 +903,8 @@ def run_serve(args, rank, world):
         rng = random.Random(int(rate) * 13 + rank)
         return [(t, kinds[k][rng.randrange(len(kinds[k]))]) for t, k in zip(arr, kk)]
 
-    def run_session(tr):
-        sess = serve.Session(n_streams=8)
+    def run_session(tr, heavy_work=0.0):
+        sess = serve.Session(n_streams=8, heavy_work=heavy_work)
         t0 = sess.clock_ms()
         pending = collections.deque()
         lat, mismatches, checked = [], 0, 0
@@ -973,7 +973,8 @@ def run_serve(args, rank, world):
     with ClockSampler(dev) as clk:
         for rate in workloads.SERVE_RATES:
             tr = trace(float(rate))
-            rates[str(rate)] = {"served": run_session(tr), "plain": run_plain(tr)}
+            rates[str(rate)] = {"served": run_session(tr), "served_heavy_lowprio": run_session(tr, 1e9),
+                                "plain": run_plain(tr)}
     top = rates[str(workloads.SERVE_RATES[-1])]
     # value: the highest offered rate's served throughput
     res = {"metric": SERVE_METRIC, "value": top["served"]["queries_per_s"], "unit": "queries/s", "n_gpus": world,

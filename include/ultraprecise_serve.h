@@ -25,10 +25,12 @@ extern "C" {
 typedef struct up_serve up_serve;
 
 typedef struct up_serve_opts {
-    int32_t n_streams;         /* concurrent launch streams (0 = 8) */
+    int32_t n_streams;         /* launch streams in total, a quarter of them for heavy requests (0 = 8) */
     int32_t max_inflight;      /* launched, not yet completed (0 = 1024) */
     int64_t memory_cap_bytes;  /* cap on outstanding request memory (0 = the free-memory budget) */
     int64_t reserve_bytes;     /* device memory left free (0 = 2 GiB) */
+    double heavy_work;         /* > 0: estimated limb work (rows x per-row work) above which a request runs on a
+                                  low-priority stream with one CTA per tile; <= 0: off (all streams equal) */
 } up_serve_opts;
 
 typedef struct up_serve_request {

@@ -42,9 +42,6 @@ struct Req {
 };
 
 constexpr int64_t kAlign = 256;
-// Requests whose estimated limb work (rows x per-row work) exceeds this run on
-// low-priority streams with one CTA per tile; the rest on high-priority streams.
-constexpr double kHeavyWork = 1e9;
 int64_t pad(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 }  // namespace
@@ -95,7 +92,7 @@ void CUDART_CB on_done(void* p) {
 
 // Bytes a request needs while it runs: its outputs (plus the err slot) and,
 // for queries, the accumulator scratch up_query_launch allocates.
-void size_request(Req& r) {
+void size_request(Req& r, double heavy_work) {
     const GeneratedModule& g = r.module->jm.gen;
     r.part_off.clear();
     r.part_bytes.clear();
@@ -116,7 +113,7 @@ void size_request(Req& r) {
         r.bytes = off + pad((int64_t)r.n_groups * accw * 4 + 16) + pad((int64_t)r.n_groups * 8);
     }
     r.out_bytes = off;
-    r.heavy = (double)r.rows * (double)g.work_per_row > kHeavyWork;
+    r.heavy = heavy_work > 0 && (double)r.rows * (double)g.work_per_row > heavy_work;
 }
 
 // Launch one admitted request on its stream (scheduler thread, lock not held).
@@ -224,10 +221,13 @@ up_status up_serve_create(const up_serve_opts* opts, up_serve** out) {
     if (s->opts.memory_cap_bytes > 0) s->budget = std::min(s->budget, s->opts.memory_cap_bytes);
     int least = 0, greatest = 0;
     cudaDeviceGetStreamPriorityRange(&least, &greatest);
-    const int n_heavy = std::max(1, s->opts.n_streams / 4);
-    for (int i = 0; i < s->opts.n_streams + n_heavy; i++) {
+    // n_streams in total (the hardware has 8 work queues by default; more
+    // streams alias onto them): a quarter low-priority for heavy requests
+    const int n_heavy = s->opts.heavy_work > 0 ? std::max(1, s->opts.n_streams / 4) : 0;
+    const int n_light = std::max(1, s->opts.n_streams - n_heavy);
+    for (int i = 0; i < n_light + n_heavy; i++) {
         cudaStream_t st;
-        const bool hv = i >= s->opts.n_streams;
+        const bool hv = i >= n_light;
         if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hv ? least : greatest) != cudaSuccess) {
             cudaGetLastError();
             for (auto x : s->streams) cudaStreamDestroy(x);
@@ -263,7 +263,7 @@ up_status up_serve_submit(up_serve* s, const up_serve_request* req, int64_t* id)
     r->group_ids = req->group_ids;
     r->n_groups = req->n_groups;
     r->owner = s;
-    size_request(*r);
+    size_request(*r, s->opts.heavy_work);
     std::lock_guard<std::mutex> g(s->mu);
     if (r->bytes > s->budget) return fail(UP_ERR_NO_MEMORY, "request larger than the session's memory budget");
     r->arrival_ms = req->arrival_ms >= 0 ? req->arrival_ms : s->now_ms();

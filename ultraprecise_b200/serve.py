@@ -16,7 +16,7 @@ QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
 
 class UpServeOpts(C.Structure):
     _fields_ = [("n_streams", C.c_int32), ("max_inflight", C.c_int32), ("memory_cap_bytes", C.c_int64),
-                ("reserve_bytes", C.c_int64)]
+                ("reserve_bytes", C.c_int64), ("heavy_work", C.c_double)]
 
 
 class UpServeRequest(C.Structure):
@@ -53,9 +53,9 @@ def percentiles(lat_ms: Sequence[float]):
 
 class Session:
     def __init__(self, n_streams: int = 0, max_inflight: int = 0, memory_cap_bytes: int = 0,
-                 reserve_bytes: int = 0):
+                 reserve_bytes: int = 0, heavy_work: float = 0.0):
         lib = abi.load()
-        o = UpServeOpts(n_streams, max_inflight, memory_cap_bytes, reserve_bytes)
+        o = UpServeOpts(n_streams, max_inflight, memory_cap_bytes, reserve_bytes, heavy_work)
         h = C.c_void_p()
         abi.check(lib.up_serve_create(C.byref(o), C.byref(h)), "up_serve_create")
         self._h = h
