@@ -34,7 +34,7 @@ struct Req {
     int64_t bytes = 0;                  // outputs + query scratch, for admission
     std::vector<int64_t> part_off, part_bytes;
     int64_t out_bytes = 0;              // the allocation: err word slot + outputs
-    bool heavy = false;                 // estimated work above kHeavyWork: low-priority stream, spread grid
+    bool heavy = false;                 // work above opts.heavy_work: low-priority stream, spread grid
     void* mem = nullptr;
     cudaStream_t stream = nullptr;
     uint32_t* host_err = nullptr;       // pinned slot the err word is copied to
