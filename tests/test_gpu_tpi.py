@@ -1,0 +1,95 @@
+"""GPU parity of the cooperative evaluation (several threads per value,
+carries passed by warp shuffles) against the oracle and the one-thread path,
+byte for byte, for every group size."""
+import random
+
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from oracle import oracle
+from tests.helpers import edge_values
+from ultraprecise_b200 import abi, codec, runtime
+from ultraprecise_b200 import expr as E
+
+pytestmark = pytest.mark.gpu
+
+
+def _exprs():
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    return {
+        "mad": a * b + c,
+        "msub": a - b * c,
+        "addsub": (a + b) - (c - a),
+        "const": a * E.dec("-12345678901234567890.123") + E.lit(7) * b,
+    }
+
+
+def _columns(p, rows, seed):
+    """Edge and random values; every 7th row of column 1 repeats column 0 so
+    that sums of opposite signs cancel to +0."""
+    rng = random.Random(seed)
+    v0 = edge_values(p, rng, rows)
+    v1 = [v0[i] if i % 7 == 0 else x for i, x in enumerate(edge_values(p, rng, rows))]
+    v2 = edge_values(p, rng, rows)
+    return [v0, v1, v2]
+
+
+def _run(e, types, raws, rows, tpv):
+    m = runtime.compile_expr(e, types, threads_per_value=tpv)
+    dev = [runtime.DeviceColumn.from_host(r, t.precision, t.scale) for r, t in zip(raws, types)]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = m.launch(dev, rows, err=err)
+    torch.cuda.synchronize()
+    return bytes(out.cpu().numpy().tobytes()), int(err.item())
+
+
+def _oracle(e, types, raws, rows):
+    b = E.build([e], types)
+    E.derive_types(b)
+    root = b.nodes[b.roots[0]]
+    ob = 1 if root.kind in abi.COMPARE_KINDS else codec.compact_bytes(root.precision)
+    return oracle.eval_expr(b, b.roots[0], raws, rows, ob, threads=8)
+
+
+@pytest.mark.parametrize("p", [76, 150, 600])
+@pytest.mark.parametrize("name", ["mad", "msub", "addsub", "const"])
+def test_cooperative_matches_oracle(p, name):
+    s = p // 4
+    e = _exprs()[name]
+    types = [E.ColType(p, s)] * 3
+    rows = 3001
+    raws = [codec.encode(v, p) for v in _columns(p, rows, seed=p * 31 + len(name))]
+    exp, exp_err = _oracle(e, types, raws, rows)
+    for tpv in (0, 2, 8, 32):
+        got, err = _run(e, types, raws, rows, tpv)
+        assert got == exp, f"threads_per_value={tpv}"
+        assert err == exp_err
+
+
+@pytest.mark.parametrize("p", [150, 300])
+def test_cooperative_products_rescale_compare(p):
+    s = p // 5
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    types = [E.ColType(p, s), E.ColType(p // 2, s // 2), E.ColType(p, s)]
+    rows = 2000
+    vals = _columns(p // 2, rows, seed=p)  # every value fits the narrowest column
+    raws = [codec.encode(v, t.precision) for v, t in zip(vals, types)]
+    for e in (a * b * c, E.rescale(a * b, 3 * p, s + s // 2 + 5), E.Expr(abi.UP_NODE_GE, a * b, c),
+              E.Expr(abi.UP_NODE_EQ, a, c)):
+        exp, exp_err = _oracle(e, types, raws, rows)
+        one, _ = _run(e, types, raws, rows, 1)
+        assert one == exp
+        for tpv in (4, 16, 32):
+            got, err = _run(e, types, raws, rows, tpv)
+            assert got == exp and err == exp_err, f"threads_per_value={tpv}"
+
+
+def test_automatic_choice_of_cooperative_path():
+    """The widest a*b+c sweep expression compiles to the cooperative kernel,
+    narrower ones to one thread per value."""
+    from ultraprecise_b200 import workloads
+    for p, coop in ((150, False), (300, False), (600, True)):
+        e, cols = workloads.sweep_expr(p, "mad")
+        src = runtime.compile_expr(e, cols).source()
+        assert ("up_trow" in src) == coop, p

@@ -153,9 +153,45 @@ UP_DI void add_signed(u32 (&r)[N], u32& sr, const u32 (&a)[NA], u32 sa, const u3
     sr = same ? sa : (nz ? (neg ? sb : (sb ^ 1u)) : 0u);
 }
 
+// r = a * b (low N limbs of the product), column by column: limb k of the
+// result is the sum of a[i]*b[k-i], final once written, so operand limbs die
+// as the columns pass them and no partial-result array stays live (fully
+// unrolled sizes).  Each column is summed in four independent chains (low and
+// high product halves, even and odd i), 64-bit each, so consecutive products
+// do not wait on one another: a column of up to 2^20 products stays below 2^52
+// per chain and the carry into the next column below 2^54.
+template <int N, int NA, int NB>
+UP_DI void mul_columns(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
+    u64 carry = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const int i0 = k - (NB - 1) > 0 ? k - (NB - 1) : 0;
+        const int i1 = k < NA - 1 ? k : NA - 1;
+        u64 lo0 = 0, lo1 = 0, hi0 = 0, hi1 = 0;
+#pragma unroll
+        for (int i = i0; i <= i1; i++) {
+            const u64 p = (u64)a[i] * b[k - i];
+            if ((i & 1) == 0) {
+                lo0 += (u32)p;
+                hi0 += p >> 32;
+            } else {
+                lo1 += (u32)p;
+                hi1 += p >> 32;
+            }
+        }
+        const u64 col = lo0 + lo1 + carry;
+        r[k] = (u32)col;
+        carry = (col >> 32) + hi0 + hi1;
+    }
+}
+
 // r = a * b (low N limbs of the product)
 template <int N, int NA, int NB>
 UP_DI void mul(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
+    if constexpr (NA * NB <= kMulUnrollPairs && NA > 1 && NB > 1) {
+        mul_columns(r, a, b);
+        return;
+    }
     zero(r);
     // products above UP_MUL_UNROLL_PAIRS limb pairs keep the outer loop rolled
     // (compile time)
@@ -558,6 +594,315 @@ UP_DI u32 st_compact_words(u8* p, const u32 (&m)[N], u32 sign) {
         w[i] = v;
     }
     return compact_overflow<B>(m);
+}
+
+// ------------------------------------------------ cooperative values
+// T threads (T a power of two dividing 32; a group is T consecutive lanes of
+// one warp) hold one value: the thread of rank g holds limbs [g*K, g*K + K).
+// Carries and borrows between threads move by warp shuffles and ballots.
+// Every shuffle and ballot below runs on all 32 lanes with the same control
+// flow (callers keep whole warps converged: a group without a row works on
+// zeros and skips its stores).
+constexpr u32 kFull = 0xffffffffu;
+
+template <int T>
+UP_DI int tpi_rank() { return (int)(threadIdx.x & (T - 1)); }
+
+template <int T>
+UP_DI u32 tpi_ballot(bool p) {
+    const u32 b = __ballot_sync(kFull, p);
+    if constexpr (T == 32) return b;
+    else return (b >> ((threadIdx.x & 31u) & ~(u32)(T - 1))) & ((1u << T) - 1u);
+}
+
+// Carry into each thread from per-thread generate (a carry leaves the
+// thread regardless of its input) and propagate (an incoming carry passes
+// through) flags: the carries of the binary sum (G|P) + G.
+template <int T>
+UP_DI u32 tpi_carry_in(bool gen, bool prop) {
+    const u32 G = tpi_ballot<T>(gen);
+    const u32 A = G | tpi_ballot<T>(prop);
+    const u32 cin = (A + G) ^ A ^ G;
+    return (cin >> tpi_rank<T>()) & 1u;
+}
+
+// x += cin (0 or 1) at this thread's lowest limb
+template <int K>
+UP_DI void tpi_inc_local(u32 (&x)[K], u32 cin) {
+    u32 c = cin;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const u32 t = x[i] + c;
+        c = (c != 0u && t == 0u) ? 1u : 0u;
+        x[i] = t;
+    }
+}
+
+// r = a + b (magnitudes; the carry out of the top thread is dropped)
+template <int T, int K>
+UP_DI void tpi_add(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K]) {
+    u64 c = 0;
+    u32 all = kFull;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        c += (u64)a[i] + b[i];
+        r[i] = (u32)c;
+        c >>= 32;
+        all &= r[i];
+    }
+    tpi_inc_local(r, tpi_carry_in<T>(c != 0, all == kFull));
+}
+
+// r = a - b for magnitudes a >= b
+template <int T, int K>
+UP_DI void tpi_sub(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K]) {
+    u64 br = 0;
+    u32 any = 0;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const u64 d = (u64)a[i] - b[i] - br;
+        r[i] = (u32)d;
+        br = d >> 63;
+        any |= r[i];
+    }
+    u32 bin = tpi_carry_in<T>(br != 0, any == 0u);
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const u32 t = r[i] - bin;
+        bin = (bin != 0u && r[i] == 0u) ? 1u : 0u;
+        r[i] = t;
+    }
+}
+
+// Magnitude comparison: -1, 0 or 1 on every thread of the group.
+template <int T, int K>
+UP_DI int tpi_cmp(const u32 (&a)[K], const u32 (&b)[K]) {
+    int lc = 0;
+#pragma unroll
+    for (int i = K - 1; i >= 0; i--)
+        if (lc == 0 && a[i] != b[i]) lc = a[i] > b[i] ? 1 : -1;
+    const u32 m = tpi_ballot<T>(lc != 0);
+    const int top = m ? 31 - __clz((int)m) : 0;
+    const int v = __shfl_sync(kFull, lc, top, T);
+    return m ? v : 0;
+}
+
+template <int T, int K>
+UP_DI bool tpi_is_zero(const u32 (&a)[K]) {
+    u32 o = 0;
+#pragma unroll
+    for (int i = 0; i < K; i++) o |= a[i];
+    return tpi_ballot<T>(o != 0u) == 0u;
+}
+
+// Signed add with the sign rules of add_signed (equal magnitudes of opposite
+// sign give +0).
+template <int T, int K>
+UP_DI void tpi_add_signed(u32 (&r)[K], u32& sr, const u32 (&a)[K], u32 sa, const u32 (&b)[K], u32 sb) {
+    const int c = tpi_cmp<T, K>(a, b);
+    u32 x[K], y[K], sum[K], dif[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        x[i] = c >= 0 ? a[i] : b[i];
+        y[i] = c >= 0 ? b[i] : a[i];
+    }
+    tpi_add<T, K>(sum, a, b);
+    tpi_sub<T, K>(dif, x, y);
+    const bool same = sa == sb;
+#pragma unroll
+    for (int i = 0; i < K; i++) r[i] = same ? sum[i] : dif[i];
+    sr = same ? sa : (c == 0 ? 0u : (c > 0 ? sa : sb));
+}
+
+// Signed comparison with the rules of compare (-0 < +0).
+template <int T, int K>
+UP_DI u32 tpi_compare(int op, const u32 (&a)[K], u32 sa, const u32 (&b)[K], u32 sb) {
+    const int c = tpi_cmp<T, K>(a, b);
+    bool lt, gt, eq;
+    if (sa != sb) {
+        lt = sa == 1u;
+        gt = sa == 0u;
+        eq = false;
+    } else {
+        eq = c == 0;
+        lt = sa == 0u ? c < 0 : c > 0;
+        gt = sa == 0u ? c > 0 : c < 0;
+    }
+    switch (op) {
+        case 0: return lt;
+        case 1: return !gt;
+        case 2: return gt;
+        case 3: return !lt;
+        case 4: return eq;
+        default: return !eq;
+    }
+}
+
+// Window bookkeeping shared by the two multiplies: after the streamed steps
+// the window holds product limbs LB.. (relative position 0 at thread 0,
+// limb 0) with one pending carry bit per thread owed to the next thread;
+// resolve the bits and move the window to absolute positions >= LB of r.
+template <int T, int K, int LB>
+UP_DI void tpi_window_out(u32 (&r)[K], u32 (&acc)[K], u32 e) {
+    const int g = tpi_rank<T>();
+    u32 ein = __shfl_up_sync(kFull, e, 1, T);
+    if (g == 0) ein = 0u;
+    u32 c = ein, all = kFull;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const u32 t = acc[i] + c;
+        c = (c != 0u && t == 0u) ? 1u : 0u;
+        acc[i] = t;
+        all &= t;
+    }
+    tpi_inc_local(acc, tpi_carry_in<T>(c != 0u, all == kFull));
+    constexpr int q = LB / K, rr = LB % K;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int src = i >= rr ? i - rr : i - rr + K;
+        const int d = i >= rr ? q : q + 1;
+        if (d < T) {
+            const u32 v = __shfl_up_sync(kFull, acc[src], d, T);
+            if (g >= d && g * K + i >= LB) r[i] = v;
+        }
+    }
+}
+
+// r = a * b (low T*K limbs); only the first LB limbs of b may be nonzero.
+// A window of T*K limbs slides over the product: at step j every thread adds
+// a_local * b_j into its window limbs, the lowest limb (product limb j) is
+// final and goes to its owner, and the window moves down one limb.
+template <int T, int K, int LB>
+UP_DI void tpi_mul(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K]) {
+    const int g = tpi_rank<T>();
+    u32 acc[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        acc[i] = 0u;
+        r[i] = 0u;
+    }
+    u32 e = 0u;
+#pragma unroll
+    for (int j = 0; j < LB; j++) {
+        const u32 bj = __shfl_sync(kFull, b[j % K], j / K, T);
+        u32 ein = __shfl_up_sync(kFull, e, 1, T);
+        if (g == 0) ein = 0u;
+        u64 c = ein;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const u64 t = (u64)a[i] * bj + acc[i] + c;
+            acc[i] = (u32)t;
+            c = t >> 32;
+        }
+        const u32 out = __shfl_sync(kFull, acc[0], 0, T);
+        if (g == j / K) r[j % K] = out;
+        u32 nx = __shfl_down_sync(kFull, acc[0], 1, T);
+        if (g == T - 1) nx = 0u;
+#pragma unroll
+        for (int i = 0; i < K - 1; i++) acc[i] = acc[i + 1];
+        const u64 top = (u64)nx + c;
+        acc[K - 1] = (u32)top;
+        e = (u32)(top >> 32);
+    }
+    tpi_window_out<T, K, LB>(r, acc, e);
+}
+
+// r = a * p for a static multiplier p of NP limbs (alignment by 10^d).
+template <int T, int K, int NP>
+UP_DI void tpi_mul_const(u32 (&r)[K], const u32 (&a)[K], const u32 (&p)[NP]) {
+    const int g = tpi_rank<T>();
+    u32 acc[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        acc[i] = 0u;
+        r[i] = 0u;
+    }
+    u32 e = 0u;
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+        u32 ein = __shfl_up_sync(kFull, e, 1, T);
+        if (g == 0) ein = 0u;
+        u64 c = ein;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const u64 t = (u64)a[i] * p[j] + acc[i] + c;
+            acc[i] = (u32)t;
+            c = t >> 32;
+        }
+        const u32 out = __shfl_sync(kFull, acc[0], 0, T);
+        if (g == j / K) r[j % K] = out;
+        u32 nx = __shfl_down_sync(kFull, acc[0], 1, T);
+        if (g == T - 1) nx = 0u;
+#pragma unroll
+        for (int i = 0; i < K - 1; i++) acc[i] = acc[i + 1];
+        const u64 top = (u64)nx + c;
+        acc[K - 1] = (u32)top;
+        e = (u32)(top >> 32);
+    }
+    tpi_window_out<T, K, NP>(r, acc, e);
+}
+
+// A distributed copy of a constant held in device memory (nl limbs).
+template <int T, int K>
+UP_DI void tpi_const(u32 (&x)[K], const u32* __restrict__ c, int nl) {
+    const int g = tpi_rank<T>();
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int l = g * K + i;
+        x[i] = l < nl ? c[l] : 0u;
+    }
+}
+
+// Compact value of B bytes -> this thread's K limbs and the sign.
+template <int T, int K, int B>
+UP_DI void tpi_ld(const u8* __restrict__ p, u32 (&x)[K], u32& sign) {
+    const int g = tpi_rank<T>();
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int o = 4 * (g * K + i);
+        u32 w = 0u;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (o + k < B) w |= (u32)p[o + k] << (8 * k);
+        x[i] = w;
+    }
+    sign = (u32)(p[B - 1] >> 7);
+    constexpr int TOPL = (B - 1) / 4;
+    constexpr u32 CLR = ~(0x80u << (8 * ((B - 1) % 4)));
+    if (g == TOPL / K) x[TOPL % K] &= CLR;
+}
+
+// This thread's limbs -> bytes [4gK, 4gK+4K) of a B-byte compact value with
+// the sign in bit 7 of byte B-1; ERR_OVERFLOW when a magnitude bit at or
+// above 8*B-1 is set (the same rule as st_compact_bytes).  `store` false
+// computes the error word only.
+template <int T, int K, int B>
+UP_DI u32 tpi_st(u8* __restrict__ p, const u32 (&x)[K], u32 sign, bool store) {
+    const int g = tpi_rank<T>();
+    bool over = false;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int o = 4 * (g * K + i);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            u32 byte = (x[i] >> (8 * k)) & 0xffu;
+            if (o + k < B) {
+                if (o + k == B - 1) {
+                    over |= (byte & 0x80u) != 0u;
+                    byte |= sign << 7;
+                }
+                if (store) p[o + k] = (u8)byte;
+            } else {
+                over |= byte != 0u;
+            }
+        }
+    }
+    // a declared width beyond the group's limbs: zero bytes, then the sign
+    if constexpr (B > 4 * T * K) {
+        if (store)
+            for (int o = 4 * T * K + g; o < B; o += T) p[o] = (u8)(o == B - 1 ? sign << 7 : 0u);
+    }
+    return tpi_ballot<T>(over) ? ERR_OVERFLOW : 0u;
 }
 
 // ------------------------------------------------------ column access

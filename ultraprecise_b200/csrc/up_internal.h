@@ -75,6 +75,7 @@ struct GeneratedModule {
     int q_gs = 0;                 // up_query_tile_s handles n_groups <= q_gs
     int q_smem = 0;               // dynamic shared memory of the tile kernels
     long work_per_row = 0;        // limb-product work + bytes per row (scheduling cost estimate)
+    int threads_per_value = 1;    // threads cooperating on one value in the tile kernel
 };
 up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
                                int n_cols, const up_compile_opts* opts, GeneratedModule& out);
