@@ -8,6 +8,8 @@
  * (task, row tile) work items from a device queue, costliest tasks first, and
  * the whole step (queue reset, the band kernels on forked streams, the
  * aggregate finalisation) is captured once as a CUDA graph and replayed.
+ * Tasks with many rows (opts.solo_rows) run as their own per-task kernels on
+ * further forked streams of the same step, concurrently with the bands.
  * Results are byte-identical to running each task alone through
  * up_expr_launch / up_query_launch.
  */
@@ -35,6 +37,9 @@ typedef struct up_batch_opts {
     int32_t ctas_per_sm;       /* 0 = default */
     int32_t tile_rows;         /* 0 = default rows per work item */
     int32_t use_graph;         /* 1: capture the step once as a CUDA graph and replay it */
+    int32_t reserved;          /* 0 */
+    int64_t solo_rows;         /* tasks with at least this many rows run as their own kernels inside the
+                                  same step (on forked streams); 0 = 262144, < 0 = never */
 } up_batch_opts;
 
 typedef struct up_batch up_batch;

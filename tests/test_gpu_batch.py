@@ -97,7 +97,8 @@ def test_bench_tasks_without_graph_and_with_forced_shapes(bench_batch):
     tasks, data, _, exp, exp_err = bench_batch
     specs = workloads.batch_specs(tasks)
     for kw in ({"use_graph": False}, {"block_threads": 64, "ctas_per_sm": 1, "tile_rows": 256},
-               {"block_threads": 256, "ctas_per_sm": 8, "tile_rows": 4096}):
+               {"block_threads": 256, "ctas_per_sm": 8, "tile_rows": 4096},
+               {"solo_rows": 2000}, {"solo_rows": 2000, "use_graph": False}, {"solo_rows": -1}):
         b = batch.Batch(specs, **kw)
         outs, _ = _bind_all(b, tasks, data)
         err = torch.zeros(1, dtype=torch.int32, device="cuda")

@@ -20,7 +20,8 @@ class UpBatchTask(C.Structure):
 
 class UpBatchOpts(C.Structure):
     _fields_ = [("autotune", C.c_int32), ("block_threads", C.c_int32), ("ctas_per_sm", C.c_int32),
-                ("tile_rows", C.c_int32), ("use_graph", C.c_int32)]
+                ("tile_rows", C.c_int32), ("use_graph", C.c_int32), ("reserved", C.c_int32),
+                ("solo_rows", C.c_int64)]
 
 
 @dataclass
@@ -55,11 +56,12 @@ def compile_only(tasks: Sequence[TaskSpec]) -> None:
 
 class Batch:
     def __init__(self, tasks: Sequence[TaskSpec], autotune: bool = False, use_graph: bool = True,
-                 block_threads: int = 0, ctas_per_sm: int = 0, tile_rows: int = 0):
+                 block_threads: int = 0, ctas_per_sm: int = 0, tile_rows: int = 0, solo_rows: int = 0):
         lib = abi.load()
         self.specs = list(tasks)
         arr, self.built = task_array(tasks)
-        opts = UpBatchOpts(1 if autotune else 0, block_threads, ctas_per_sm, tile_rows, 1 if use_graph else 0)
+        opts = UpBatchOpts(1 if autotune else 0, block_threads, ctas_per_sm, tile_rows, 1 if use_graph else 0, 0,
+                           solo_rows)
         h = C.c_void_p()
         abi.check(lib.up_batch_create(arr, len(tasks), C.byref(opts), C.byref(h)), "up_batch_create")
         self._h = h

@@ -51,6 +51,7 @@ struct HBArgs {
 static_assert(sizeof(HBArgs) == 56, "BArgs layout");
 
 const int kThreads[3] = {64, 128, 256};
+constexpr int kSoloStreams = 1;
 
 up_status cuda_err(cudaError_t e, const std::string& what) {
     cudaGetLastError();
@@ -92,6 +93,15 @@ uint64_t fnv(const std::string& s) {
 
 struct up_batch {
     GeneratedBatch gen;
+    // per task: a copy of its typed tree (for the per-task module of a solo task)
+    std::vector<std::vector<up_expr_node>> t_nodes;
+    std::vector<std::vector<up_col_type>> t_cols;
+    std::vector<int> t_root, t_agg;
+    std::vector<std::vector<up_column>> t_in;  // bound columns
+    std::vector<bool> solo;                    // runs as its own kernel this step
+    std::vector<up_module*> solo_mod;
+    cudaStream_t solo_side[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t solo_join[4] = {nullptr, nullptr, nullptr, nullptr};
     std::shared_ptr<JitKernelSet> ks;
     up_batch_opts opts{};
     std::vector<HBTask> host_tasks;
@@ -137,6 +147,12 @@ struct up_batch {
     }
     ~up_batch() {
         drop_device();
+        for (auto* m : solo_mod)
+            if (m) up_module_release(m);
+        for (int i = 0; i < 4; i++) {
+            if (solo_side[i]) cudaStreamDestroy(solo_side[i]);
+            if (solo_join[i]) cudaEventDestroy(solo_join[i]);
+        }
         if (cap) cudaStreamDestroy(cap);
         for (int i = 0; i < 2; i++) {
             if (side[i]) cudaStreamDestroy(side[i]);
@@ -155,7 +171,7 @@ up_status build_items(up_batch* b, int band, int tile_rows) {
     if (b->items_tile_rows[band] == tile_rows && b->item_task[band]) return UP_OK;
     std::vector<int> order;
     for (size_t k = 0; k < b->gen.tasks.size(); k++)
-        if (b->gen.tasks[k].band == band && b->host_tasks[k].rows > 0) order.push_back((int)k);
+        if (b->gen.tasks[k].band == band && b->host_tasks[k].rows > 0 && !b->solo[k]) order.push_back((int)k);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->cost[x] > b->cost[y]; });
     std::vector<int32_t> it;
     std::vector<int64_t> tl;
@@ -237,9 +253,33 @@ up_status run_step(up_batch* b, uint32_t* err, cudaStream_t s) {
     if ((st = launch_band(b, 0, err, s)) != UP_OK) return st;
     if ((st = launch_band(b, 1, err, b->side[0])) != UP_OK) return st;
     if ((st = launch_band(b, 2, err, b->side[1])) != UP_OK) return st;
+    // tasks with many rows: their own kernels, one after another on a further
+    // forked stream (each fills the GPU; running them concurrently measured
+    // slower), overlapping the band kernels of the small tasks
+    int nsolo = 0;
+    for (size_t k = 0; k < b->solo.size(); k++) {
+        if (!b->solo[k]) continue;
+        const int q = nsolo++ % kSoloStreams;
+        cudaStream_t ss = b->solo_side[q];
+        if (nsolo <= kSoloStreams) UPB_CUDA(cudaStreamWaitEvent(ss, b->fork, 0));
+        const HBTask& h = b->host_tasks[k];
+        const auto& in = b->t_in[k];
+        if (b->t_agg[k] < 0) {
+            st = up_expr_launch(b->solo_mod[k], in.data(), (int32_t)in.size(), h.rows, h.out, err, ss);
+        } else {
+            void* outs[1] = {h.out};
+            st = up_query_launch(b->solo_mod[k], in.data(), (int32_t)in.size(), h.rows, h.gid, h.n_groups, outs, err,
+                                 ss);
+        }
+        if (st != UP_OK) return st;
+    }
     for (int i = 0; i < 2; i++) {
         UPB_CUDA(cudaEventRecord(b->join[i], b->side[i]));
         UPB_CUDA(cudaStreamWaitEvent(s, b->join[i], 0));
+    }
+    for (int q = 0; q < std::min(nsolo, kSoloStreams); q++) {
+        UPB_CUDA(cudaEventRecord(b->solo_join[q], b->solo_side[q]));
+        UPB_CUDA(cudaStreamWaitEvent(s, b->solo_join[q], 0));
     }
     return launch_fin(b, err, s);
 }
@@ -247,12 +287,30 @@ up_status run_step(up_batch* b, uint32_t* err, cudaStream_t s) {
 up_status prepare(up_batch* b) {
     if (b->prepared) return UP_OK;
     const size_t nt = b->host_tasks.size();
+    // tasks with many rows run as their own per-task kernels
+    const int64_t solo_rows = b->opts.solo_rows == 0 ? (int64_t)262144 : b->opts.solo_rows;
+    for (size_t k = 0; k < nt; k++) {
+        b->solo[k] = solo_rows > 0 && b->host_tasks[k].rows >= solo_rows;
+        if (!b->solo[k] || b->solo_mod[k]) continue;
+        up_module* m = nullptr;
+        up_status st;
+        if (b->t_agg[k] < 0) {
+            st = up_module_compile(b->t_nodes[k].data(), (int32_t)b->t_nodes[k].size(), b->t_root[k],
+                                   b->t_cols[k].data(), (int32_t)b->t_cols[k].size(), nullptr, &m);
+        } else {
+            up_query_agg qa = {b->t_agg[k], b->t_root[k]};
+            st = up_query_compile(b->t_nodes[k].data(), (int32_t)b->t_nodes[k].size(), b->t_cols[k].data(),
+                                  (int32_t)b->t_cols[k].size(), &qa, 1, nullptr, &m);
+        }
+        if (st != UP_OK) return st;
+        b->solo_mod[k] = m;
+    }
     size_t off = 0;
     std::vector<size_t> acc_off(nt, 0), cnt_off(nt, 0);
     b->max_groups = 0;
     for (size_t k = 0; k < nt; k++) {
         const auto& gt = b->gen.tasks[k];
-        if (gt.agg < 0) continue;
+        if (gt.agg < 0 || b->solo[k]) continue;
         const int G = b->host_tasks[k].n_groups;
         b->max_groups = std::max(b->max_groups, G);
         acc_off[k] = off;
@@ -262,32 +320,30 @@ up_status prepare(up_batch* b) {
     }
     b->scratch_bytes = off;
     if (off) UPB_CUDA(cudaMalloc(&b->scratch, off));
+    std::vector<HBTask> dev_tasks = b->host_tasks;
     for (size_t k = 0; k < nt; k++) {
+        if (b->solo[k]) {  // neither the bands nor the finalisation touch it
+            dev_tasks[k].rows = 0;
+            dev_tasks[k].n_groups = 0;
+            continue;
+        }
         if (b->gen.tasks[k].agg < 0) continue;
-        b->host_tasks[k].acc = (uint32_t*)((uint8_t*)b->scratch + acc_off[k]);
-        b->host_tasks[k].cnt = (uint64_t*)((uint8_t*)b->scratch + cnt_off[k]);
+        dev_tasks[k].acc = (uint32_t*)((uint8_t*)b->scratch + acc_off[k]);
+        dev_tasks[k].cnt = (uint64_t*)((uint8_t*)b->scratch + cnt_off[k]);
     }
     UPB_CUDA(cudaMalloc(&b->d_tasks, nt * sizeof(HBTask)));
-    UPB_CUDA(cudaMemcpy(b->d_tasks, b->host_tasks.data(), nt * sizeof(HBTask), cudaMemcpyHostToDevice));
+    UPB_CUDA(cudaMemcpy(b->d_tasks, dev_tasks.data(), nt * sizeof(HBTask), cudaMemcpyHostToDevice));
     UPB_CUDA(cudaMalloc((void**)&b->heads, 3 * sizeof(unsigned long long)));
     for (int i = 0; i < 2; i++) {
         if (!b->side[i]) UPB_CUDA(cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking));
         if (!b->join[i]) UPB_CUDA(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming));
     }
+    for (int i = 0; i < 4; i++) {
+        if (!b->solo_side[i]) UPB_CUDA(cudaStreamCreateWithFlags(&b->solo_side[i], cudaStreamNonBlocking));
+        if (!b->solo_join[i]) UPB_CUDA(cudaEventCreateWithFlags(&b->solo_join[i], cudaEventDisableTiming));
+    }
     if (!b->fork) UPB_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     if (!b->cap) UPB_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
-    // Task functions are called (not inlined), so wide bands keep their limb
-    // arrays in a stack frame of a few KB per thread; the linker sizes it
-    // statically, and the context's per-thread stack limit is raised to match.
-    size_t need = 0;
-    for (const auto& name : b->gen.kernels) {
-        void* k = jit_kernel(*b->ks, name);
-        cudaFuncAttributes fa;
-        if (k && cudaFuncGetAttributes(&fa, (const void*)k) == cudaSuccess) need = std::max(need, fa.localSizeBytes);
-    }
-    size_t have = 0;
-    UPB_CUDA(cudaDeviceGetLimit(&have, cudaLimitStackSize));
-    if (need > have) UPB_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, (need + 255) & ~size_t(255)));
     for (int band = 0; band < 3; band++) {
         up_status st = build_items(b, band, b->shape[band].tile_rows);
         if (st != UP_OK) return st;
@@ -351,7 +407,7 @@ up_status autotune(up_batch* b, cudaStream_t s) {
     for (int band = 0; band < 3 && st == UP_OK; band++) {
         bool any = false;
         for (size_t k = 0; k < b->gen.tasks.size(); k++)
-            if (b->gen.tasks[k].band == band && b->host_tasks[k].rows > 0) any = true;
+            if (b->gen.tasks[k].band == band && b->host_tasks[k].rows > 0 && !b->solo[k]) any = true;
         if (!any) continue;
         Shape best = b->shape[band];
         best.tuned_ms = 1e30;
@@ -414,6 +470,15 @@ up_status up_batch_create(const up_batch_task* tasks, int32_t n_tasks, const up_
     memset(b->host_tasks.data(), 0, sizeof(HBTask) * n_tasks);
     b->bound.assign(n_tasks, false);
     b->cost.assign(n_tasks, 1.0);
+    b->solo.assign(n_tasks, false);
+    b->solo_mod.assign(n_tasks, nullptr);
+    b->t_in.assign(n_tasks, {});
+    for (int k = 0; k < n_tasks; k++) {
+        b->t_nodes.emplace_back(tasks[k].nodes, tasks[k].nodes + tasks[k].n_nodes);
+        b->t_cols.emplace_back(tasks[k].cols, tasks[k].cols + tasks[k].n_cols);
+        b->t_root.push_back(tasks[k].root);
+        b->t_agg.push_back(tasks[k].agg_kind);
+    }
     for (int k = 0; k < n_tasks; k++) {
         // per-row cost estimate: limb products of every node
         std::vector<NodeFacts> f;
@@ -457,6 +522,7 @@ up_status up_batch_bind(up_batch* b, int32_t task, const up_column* in, int32_t 
         h.col[c].value_bytes = in[c].value_bytes;
         if (((uintptr_t)in[c].data & 3u) != 0) words = false;
     }
+    b->t_in[task].assign(in, in + gt.in_bytes.size());
     h.rows = rows;
     h.out = (uint8_t*)out;
     h.gid = group_ids;

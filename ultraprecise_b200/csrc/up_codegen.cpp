@@ -256,8 +256,8 @@ struct TEmitter {
         const int d = sc - f[a].scale;
         const Big p = big_pow10(d);
         std::string t = "t" + std::to_string(tmp++);
-        body << "    u32 " << t << "[" << K << "]; tpi_mul_const<" << tk() << ", " << p.m.size() << ">(" << t << ", "
-             << v(a) << ", " << p10_name(d) << ");\n";
+        body << "    u32 " << t << "[" << K << "]; tpi_mul_const<" << tk() << ", " << f[a].limbs << ", " << p.m.size()
+             << ">(" << t << ", " << v(a) << ", " << p10_name(d) << ");\n";
         return t;
     }
     void constant(int k, const Big& c, uint32_t sign) {
@@ -305,7 +305,8 @@ struct TEmitter {
                 // the operand with fewer limbs is streamed limb by limb
                 int a = nd.left, b = nd.right;
                 if (f[a].limbs < f[b].limbs) std::swap(a, b);
-                body << "    u32 " << v(k) << "[" << K << "]; tpi_mul<" << tk() << ", " << f[b].limbs << ">(" << v(k)
+                body << "    u32 " << v(k) << "[" << K << "]; tpi_mul<" << tk() << ", " << f[a].limbs << ", " << f[b].limbs
+                     << ">(" << v(k)
                      << ", " << v(a) << ", " << v(b) << "); u32 " << s(k) << " = " << s(nd.left) << " ^ "
                      << s(nd.right) << ";\n";
                 break;

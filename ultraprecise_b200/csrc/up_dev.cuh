@@ -738,108 +738,132 @@ UP_DI u32 tpi_compare(int op, const u32 (&a)[K], u32 sa, const u32 (&b)[K], u32 
     }
 }
 
-// Window bookkeeping shared by the two multiplies: after the streamed steps
-// the window holds product limbs LB.. (relative position 0 at thread 0,
-// limb 0) with one pending carry bit per thread owed to the next thread;
-// resolve the bits and move the window to absolute positions >= LB of r.
-template <int T, int K, int LB>
-UP_DI void tpi_window_out(u32 (&r)[K], u32 (&acc)[K], u32 e) {
+// Multiplication streams one operand limb by limb through a window that
+// holds the running partial product of the other operand a (LA nonzero
+// limbs).  The window needs LA+1 limbs, so it uses KA limbs per thread, the
+// smallest divisor of K with T*KA >= LA+1: no thread multiplies limbs that
+// are known to be zero.
+template <int T, int K, int LA>
+__host__ __device__ constexpr int tpi_window_limbs() {
+    for (int d = 1; d <= K; d++)
+        if (K % d == 0 && T * d >= LA + 1) return d;
+    return K;
+}
+
+// a in the K-limb layout -> the KA-limb layout (KA divides K)
+template <int T, int K, int KA>
+UP_DI void tpi_pack(u32 (&aw)[KA], const u32 (&a)[K]) {
+    if constexpr (KA == K) {
+#pragma unroll
+        for (int i = 0; i < K; i++) aw[i] = a[i];
+    } else {
+        const int g = tpi_rank<T>();
+        const int sel = ((g * KA) % K) / KA;
+#pragma unroll
+        for (int i = 0; i < KA; i++) {
+            const int src = (g * KA + i) / K;
+            u32 v = 0u;
+#pragma unroll
+            for (int m = 0; m < K / KA; m++) {
+                const u32 t = __shfl_sync(kFull, a[m * KA + i], src, T);
+                if (sel == m) v = t;
+            }
+            aw[i] = v;
+        }
+    }
+}
+
+// One window step: acc += a * bj (pending carry bits e from the thread
+// below enter at limb 0); returns product limb j (final, from rank 0) and
+// moves the window down one limb.
+template <int T, int KA>
+UP_DI u32 tpi_window_step(u32 (&acc)[KA], u32& e, const u32 (&aw)[KA], u32 bj) {
+    const int g = tpi_rank<T>();
+    u32 ein = __shfl_up_sync(kFull, e, 1, T);
+    if (g == 0) ein = 0u;
+    u64 c = ein;
+#pragma unroll
+    for (int i = 0; i < KA; i++) {
+        const u64 t = (u64)aw[i] * bj + acc[i] + c;
+        acc[i] = (u32)t;
+        c = t >> 32;
+    }
+    const u32 out = __shfl_sync(kFull, acc[0], 0, T);
+    u32 nx = __shfl_down_sync(kFull, acc[0], 1, T);
+    if (g == T - 1) nx = 0u;
+#pragma unroll
+    for (int i = 0; i < KA - 1; i++) acc[i] = acc[i + 1];
+    const u64 top = (u64)nx + c;
+    acc[KA - 1] = (u32)top;
+    e = (u32)(top >> 32);
+    return out;
+}
+
+// After LB steps: resolve the pending carry bits and move the window (product
+// limbs LB.., KA layout) to positions >= LB of r (K layout).
+template <int T, int K, int KA, int LB>
+UP_DI void tpi_window_out(u32 (&r)[K], u32 (&acc)[KA], u32 e) {
     const int g = tpi_rank<T>();
     u32 ein = __shfl_up_sync(kFull, e, 1, T);
     if (g == 0) ein = 0u;
     u32 c = ein, all = kFull;
 #pragma unroll
-    for (int i = 0; i < K; i++) {
+    for (int i = 0; i < KA; i++) {
         const u32 t = acc[i] + c;
         c = (c != 0u && t == 0u) ? 1u : 0u;
         acc[i] = t;
         all &= t;
     }
     tpi_inc_local(acc, tpi_carry_in<T>(c != 0u, all == kFull));
-    constexpr int q = LB / K, rr = LB % K;
 #pragma unroll
     for (int i = 0; i < K; i++) {
-        const int src = i >= rr ? i - rr : i - rr + K;
-        const int d = i >= rr ? q : q + 1;
-        if (d < T) {
-            const u32 v = __shfl_up_sync(kFull, acc[src], d, T);
-            if (g >= d && g * K + i >= LB) r[i] = v;
-        }
+        const int lidx = (((i - LB) % KA) + KA) % KA;
+        const int q = g * K + i - LB;
+        const int src = q >= 0 ? q / KA : 0;
+        const u32 v = __shfl_sync(kFull, acc[lidx], src < T ? src : 0, T);
+        if (q >= 0 && src < T) r[i] = v;
     }
 }
 
-// r = a * b (low T*K limbs); only the first LB limbs of b may be nonzero.
-// A window of T*K limbs slides over the product: at step j every thread adds
-// a_local * b_j into its window limbs, the lowest limb (product limb j) is
-// final and goes to its owner, and the window moves down one limb.
-template <int T, int K, int LB>
+// r = a * b (low T*K limbs); a has at most LA nonzero limbs, b at most LB.
+template <int T, int K, int LA, int LB>
 UP_DI void tpi_mul(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K]) {
+    constexpr int KA = tpi_window_limbs<T, K, LA>();
     const int g = tpi_rank<T>();
-    u32 acc[K];
+    u32 aw[KA], acc[KA];
+    tpi_pack<T, K, KA>(aw, a);
 #pragma unroll
-    for (int i = 0; i < K; i++) {
-        acc[i] = 0u;
-        r[i] = 0u;
-    }
+    for (int i = 0; i < KA; i++) acc[i] = 0u;
+#pragma unroll
+    for (int i = 0; i < K; i++) r[i] = 0u;
     u32 e = 0u;
 #pragma unroll
     for (int j = 0; j < LB; j++) {
         const u32 bj = __shfl_sync(kFull, b[j % K], j / K, T);
-        u32 ein = __shfl_up_sync(kFull, e, 1, T);
-        if (g == 0) ein = 0u;
-        u64 c = ein;
-#pragma unroll
-        for (int i = 0; i < K; i++) {
-            const u64 t = (u64)a[i] * bj + acc[i] + c;
-            acc[i] = (u32)t;
-            c = t >> 32;
-        }
-        const u32 out = __shfl_sync(kFull, acc[0], 0, T);
+        const u32 out = tpi_window_step<T, KA>(acc, e, aw, bj);
         if (g == j / K) r[j % K] = out;
-        u32 nx = __shfl_down_sync(kFull, acc[0], 1, T);
-        if (g == T - 1) nx = 0u;
-#pragma unroll
-        for (int i = 0; i < K - 1; i++) acc[i] = acc[i + 1];
-        const u64 top = (u64)nx + c;
-        acc[K - 1] = (u32)top;
-        e = (u32)(top >> 32);
     }
-    tpi_window_out<T, K, LB>(r, acc, e);
+    tpi_window_out<T, K, KA, LB>(r, acc, e);
 }
 
 // r = a * p for a static multiplier p of NP limbs (alignment by 10^d).
-template <int T, int K, int NP>
+template <int T, int K, int LA, int NP>
 UP_DI void tpi_mul_const(u32 (&r)[K], const u32 (&a)[K], const u32 (&p)[NP]) {
+    constexpr int KA = tpi_window_limbs<T, K, LA>();
     const int g = tpi_rank<T>();
-    u32 acc[K];
+    u32 aw[KA], acc[KA];
+    tpi_pack<T, K, KA>(aw, a);
 #pragma unroll
-    for (int i = 0; i < K; i++) {
-        acc[i] = 0u;
-        r[i] = 0u;
-    }
+    for (int i = 0; i < KA; i++) acc[i] = 0u;
+#pragma unroll
+    for (int i = 0; i < K; i++) r[i] = 0u;
     u32 e = 0u;
 #pragma unroll
     for (int j = 0; j < NP; j++) {
-        u32 ein = __shfl_up_sync(kFull, e, 1, T);
-        if (g == 0) ein = 0u;
-        u64 c = ein;
-#pragma unroll
-        for (int i = 0; i < K; i++) {
-            const u64 t = (u64)a[i] * p[j] + acc[i] + c;
-            acc[i] = (u32)t;
-            c = t >> 32;
-        }
-        const u32 out = __shfl_sync(kFull, acc[0], 0, T);
+        const u32 out = tpi_window_step<T, KA>(acc, e, aw, p[j]);
         if (g == j / K) r[j % K] = out;
-        u32 nx = __shfl_down_sync(kFull, acc[0], 1, T);
-        if (g == T - 1) nx = 0u;
-#pragma unroll
-        for (int i = 0; i < K - 1; i++) acc[i] = acc[i + 1];
-        const u64 top = (u64)nx + c;
-        acc[K - 1] = (u32)top;
-        e = (u32)(top >> 32);
     }
-    tpi_window_out<T, K, NP>(r, acc, e);
+    tpi_window_out<T, K, KA, NP>(r, acc, e);
 }
 
 // A distributed copy of a constant held in device memory (nl limbs).

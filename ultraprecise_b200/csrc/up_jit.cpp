@@ -346,6 +346,28 @@ up_status jit_compile_linked(const std::vector<std::string>& units, std::vector<
     return UP_OK;
 }
 
+// Kernels that keep wide limb arrays in a stack frame may need more than the
+// context's default per-thread stack (1 KB); when they do, a launch makes the
+// driver grow local memory.  Raise the context's limit once, at load time, to
+// the largest frame of the module's kernels.
+void fit_stack_limit(const JitKernelSet& ks) {
+    static std::mutex mu;
+    size_t need = 0;
+    for (const auto& kv : ks.kernels) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, (const void*)kv.second) == cudaSuccess) need = std::max(need, fa.localSizeBytes);
+        else cudaGetLastError();
+    }
+    std::lock_guard<std::mutex> g(mu);
+    size_t have = 0;
+    if (cudaDeviceGetLimit(&have, cudaLimitStackSize) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (need > have && cudaDeviceSetLimit(cudaLimitStackSize, (need + 255) & ~(size_t)255) != cudaSuccess)
+        cudaGetLastError();
+}
+
 // Load an already compiled CUBIN and look up its kernels.
 up_status jit_load(const std::vector<char>& cubin, const std::vector<std::string>& kernels,
                    std::shared_ptr<JitKernelSet>& out) {
@@ -367,6 +389,7 @@ up_status jit_load(const std::vector<char>& cubin, const std::vector<std::string
         }
         ks->kernels[k] = h;
     }
+    fit_stack_limit(*ks);
     out = ks;
     return UP_OK;
 }
@@ -403,6 +426,7 @@ up_status jit_get(const GeneratedModule& gen, std::shared_ptr<JitKernelSet>& out
         }
         ks->kernels[k] = h;
     }
+    fit_stack_limit(*ks);
     std::lock_guard<std::mutex> g(c.mu);
     auto it = c.map.find(gen.source);
     if (it != c.map.end()) {  // another thread won the race
