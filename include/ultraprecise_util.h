@@ -47,6 +47,11 @@ up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32
 
 /* The same for a batch module (ultraprecise_batch.h): generate and compile
  * every task into one CUBIN without loading it. */
+/* Compile an expression module with explicit options (e.g. threads per
+ * value) into the cubin cache without loading it (no GPU needed). */
+up_status up_util_compile_expr_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
+                                    const up_col_type* cols, int32_t n_cols, const up_compile_opts* opts);
+
 struct up_batch_task;
 up_status up_util_compile_batch_only(const struct up_batch_task* tasks, int32_t n_tasks);
 

@@ -93,3 +93,46 @@ def test_automatic_choice_of_cooperative_path():
         e, cols = workloads.sweep_expr(p, "mad")
         src = runtime.compile_expr(e, cols).source()
         assert ("up_trow" in src) == coop, p
+
+
+def _div_exprs():
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    return {"div": a / b, "mod": a % b, "divmix": (a * c) / b + a, "trunc": E.rescale(a * b, 0, 1)}
+
+
+@pytest.mark.parametrize("p", [38, 150, 300])
+@pytest.mark.parametrize("name", ["div", "mod", "divmix", "trunc"])
+def test_cooperative_division_matches_oracle(p, name):
+    """Division in every branch of the divide rule: zero dividends and
+    divisors (edge values include zeros), small operands (the 64-bit branch),
+    one-limb divisors (remainder doubled mod 2^32), and wide divisors."""
+    s = p // 4
+    e = _div_exprs()[name]
+    if name == "trunc":
+        e = E.rescale(E.col(0) * E.col(1), 2 * p + 1, s)  # scale 2s -> s: truncation by 10^s
+    types = [E.ColType(p, s)] * 3
+    rows = 3001
+    rng = random.Random(p + len(name))
+    vals = _columns(p, rows, seed=p * 7 + len(name))
+    # small values on some rows: one-limb divisors and the 64-bit branch
+    vals[0] = [(sg, m % 10 ** 12) if i % 5 == 1 else (sg, m) for i, (sg, m) in enumerate(vals[0])]
+    vals[1] = [(sg, m % 10 ** 9) if i % 3 == 1 else (sg, m) for i, (sg, m) in enumerate(vals[1])]
+    raws = [codec.encode(v, p) for v in vals]
+    exp, exp_err = _oracle(e, types, raws, rows)
+    for tpv in (4, 8, 32):
+        got, err = _run(e, types, raws, rows, tpv)
+        assert got == exp, f"threads_per_value={tpv}"
+        assert err == exp_err
+
+
+@pytest.mark.parametrize("p,rows,tpv", [(100, 3000, 8), (300, 1500, 16), (1000, 300, 32)])
+def test_cooperative_sin_matches_oracle(p, rows, tpv):
+    from ultraprecise_b200 import workloads
+    s = p - 2
+    pi = workloads.pi_scaled(s)
+    raw = codec.encode([(0, 0), (1, 0), (0, pi), (1, pi), (0, 1)], p) + workloads.sin_inputs(p, rows - 5, seed=p)
+    e, cols = workloads.sin_expr(p)
+    exp, exp_err = _oracle(e, cols, [raw], rows)
+    got, err = _run(e, cols, [raw], rows, tpv)
+    assert got == exp
+    assert err == exp_err

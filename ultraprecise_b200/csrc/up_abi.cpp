@@ -429,6 +429,15 @@ up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32
     return jit_compile_cubin(gen.source, cubin);
 }
 
+up_status up_util_compile_expr_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
+                                    const up_col_type* cols, int32_t n_cols, const up_compile_opts* opts) {
+    GeneratedModule gen;
+    up_status st = generate_expr_module(nodes, n_nodes, root, cols, n_cols, opts, gen);
+    if (st != UP_OK) return st;
+    std::vector<char> cubin;
+    return jit_compile_cubin(gen.source, cubin);
+}
+
 up_status up_device_query(int32_t device, up_device_info* info) {
     if (!info) return fail(UP_ERR_INVALID_ARG, "info is NULL");
     memset(info, 0, sizeof *info);

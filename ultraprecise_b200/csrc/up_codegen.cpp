@@ -229,9 +229,7 @@ std::string params_decl(const std::vector<int>& used_cols) {
 }
 
 // Cooperative row code (T threads per value, K limbs per thread): the same
-// node numbering and semantics as Emitter, on the tpi_* primitives.  Used for
-// wide expressions made of loads, constants, add/sub, mul, widening rescales
-// and comparisons.
+// node numbering and semantics as Emitter, on the tpi_* primitives.
 struct TEmitter {
     const up_expr_node* nodes;
     const up_col_type* cols;
@@ -240,9 +238,24 @@ struct TEmitter {
     std::ostringstream body, globals;
     std::set<int> p10;
     int tmp = 0;
+    bool out_of_line = false;  // call multiplies and divisions out of line
 
     TEmitter(const up_expr_node* n, const up_col_type* c, const std::vector<NodeFacts>& facts, int t, int k)
         : nodes(n), cols(c), f(facts), T(t), K(k) {}
+
+    // More than this many multiplies / divisions: call them out of line, so
+    // code size (and compile time) follows the number of distinct shapes.
+    static constexpr int kOutOfLineOps = 6;
+    void plan(const std::vector<int>& topo) {
+        int ops = 0;
+        for (int k : topo) {
+            const int kind = nodes[k].kind;
+            ops += kind == UP_NODE_MUL || kind == UP_NODE_DIV ||
+                   (kind == UP_NODE_RESCALE && nodes[k].scale < f[nodes[k].left].scale);
+        }
+        out_of_line = ops > kOutOfLineOps;
+    }
+    const char* ni() const { return out_of_line ? "_ni" : ""; }
 
     std::string v(int k) { return "v" + std::to_string(k); }
     std::string s(int k) { return "s" + std::to_string(k); }
@@ -305,19 +318,46 @@ struct TEmitter {
                 // the operand with fewer limbs is streamed limb by limb
                 int a = nd.left, b = nd.right;
                 if (f[a].limbs < f[b].limbs) std::swap(a, b);
-                body << "    u32 " << v(k) << "[" << K << "]; tpi_mul<" << tk() << ", " << f[a].limbs << ", " << f[b].limbs
+                body << "    u32 " << v(k) << "[" << K << "]; tpi_mul" << ni() << "<" << tk() << ", " << f[a].limbs << ", "
+                     << f[b].limbs
                      << ">(" << v(k)
                      << ", " << v(a) << ", " << v(b) << "); u32 " << s(k) << " = " << s(nd.left) << " ^ "
                      << s(nd.right) << ";\n";
                 break;
             }
             case UP_NODE_RESCALE: {
-                const std::string A = aligned(nd.left, nd.scale);
                 body << "    u32 " << v(k) << "[" << K << "]; u32 " << s(k) << " = " << s(nd.left) << ";\n";
-                body << "#pragma unroll\n    for (int i = 0; i < " << K << "; i++) " << v(k) << "[i] = " << A
-                     << "[i];\n";
+                if (nd.scale >= f[nd.left].scale) {
+                    const std::string A = aligned(nd.left, nd.scale);
+                    body << "#pragma unroll\n    for (int i = 0; i < " << K << "; i++) " << v(k) << "[i] = " << A
+                         << "[i];\n";
+                } else {
+                    const Big p = big_pow10(f[nd.left].scale - nd.scale);
+                    globals << "__device__ const u32 R" << k << "[" << p.m.size() << "] = "
+                            << limbs_init(p, (int)p.m.size()) << ";\n";
+                    body << "    tpi_trunc_pow10" << ni() << "<" << tk() << ">(" << v(k) << ", " << v(nd.left) << ", R" << k
+                         << ", "
+                         << p.m.size() << ");\n";
+                }
                 break;
             }
+            case UP_NODE_DIV: {
+                const int sh = f[nd.right].scale + 4;
+                const Big p = big_pow10(sh);
+                char w[40];
+                snprintf(w, sizeof w, "0x%016llxull", (unsigned long long)big_low64(p));
+                body << "    u32 " << v(k) << "[" << K << "]; u32 " << s(k) << ";\n";
+                body << "    err |= tpi_div_round" << ni() << "<" << tk() << ", " << f[nd.left].limbs << ", " << p.m.size()
+                     << ", "
+                     << sh << "u, " << w << ">(" << v(k) << ", " << s(k) << ", " << v(nd.left) << ", " << s(nd.left)
+                     << ", " << v(nd.right) << ", " << s(nd.right) << ", " << p10_name(sh) << ");\n";
+                break;
+            }
+            case UP_NODE_MOD:
+                body << "    u32 " << v(k) << "[" << K << "]; u32 " << s(k) << ";\n";
+                body << "    err |= tpi_mod<" << tk() << ">(" << v(k) << ", " << s(k) << ", " << v(nd.left) << ", "
+                     << s(nd.left) << ", " << v(nd.right) << ", " << s(nd.right) << ");\n";
+                break;
             default: {
                 const int sc = std::max(f[nd.left].scale, f[nd.right].scale);
                 const std::string A = aligned(nd.left, sc);
@@ -345,8 +385,8 @@ struct TEmitter {
 constexpr int kCoopMinLimbs = 96;
 
 // Widest limb count a cooperative evaluation of the expression needs (every
-// node and every aligned operand), or 0 when a node kind has no cooperative
-// form (division, modulo, truncating rescale).
+// node, every aligned operand, and the headroom of the long divisions), or 0
+// when a node kind has no cooperative form.
 int cooperative_width(const up_expr_node* nodes, const std::vector<NodeFacts>& f, const std::vector<int>& topo) {
     int w = 1;
     for (int k : topo) {
@@ -361,12 +401,24 @@ int cooperative_width(const up_expr_node* nodes, const std::vector<NodeFacts>& f
                 w = std::max(w, f[k].limbs);
                 break;
             case UP_NODE_RESCALE:
-                if (nd.scale < f[nd.left].scale) return 0;
                 w = std::max(w, f[k].limbs);
+                if (nd.scale < f[nd.left].scale) {  // long division by 10^d: one limb of headroom each
+                    w = std::max(w, f[nd.left].limbs + 1);
+                    w = std::max(w, limbs_for_bits(big_bitlen(big_pow10(f[nd.left].scale - nd.scale))) + 1);
+                }
                 break;
-            case UP_NODE_DIV:
+            case UP_NODE_DIV: {  // dividend scaled by 10^(s_b+4), plus headroom for normalising
+                const int np = (int)big_pow10(f[nd.right].scale + 4).m.size();
+                w = std::max(w, f[k].limbs);
+                w = std::max(w, f[nd.left].limbs + np + 1);
+                w = std::max(w, f[nd.right].limbs + 1);
+                break;
+            }
             case UP_NODE_MOD:
-                return 0;
+                w = std::max(w, f[k].limbs);
+                w = std::max(w, f[nd.left].limbs + 1);
+                w = std::max(w, f[nd.right].limbs + 1);
+                break;
             default:
                 if (!is_compare_kind(nd.kind)) return 0;
                 {
@@ -453,7 +505,14 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     {
         const int req = opts ? opts->threads_per_value : 0;
         const int w = cooperative_width(nodes, f, topo);
-        if (w > 0 && req != 1 && !any_nullable && (req > 1 || w >= kCoopMinLimbs)) {
+        // divisions run cooperatively only on request: measured on B200, one
+        // thread per value divides 2-5x faster (each long-division step costs
+        // the group several broadcasts and ballots)
+        bool has_div = false;
+        for (int k : topo)
+            has_div |= nodes[k].kind == UP_NODE_DIV || nodes[k].kind == UP_NODE_MOD ||
+                       (nodes[k].kind == UP_NODE_RESCALE && nodes[k].scale < f[nodes[k].left].scale);
+        if (w > 0 && req != 1 && !any_nullable && (req > 1 || (w >= kCoopMinLimbs && !has_div))) {
             if (req > 1) {
                 tpiT = req;
             } else {
@@ -471,6 +530,7 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     int smem = 0;
     if (tpiT > 0) {
         TEmitter te(nodes, cols, f, tpiT, tpiK);
+        te.plan(topo);
         for (int k : topo) te.node(k);
         const int CT = 256;               // CTA threads
         const int G = CT / tpiT;          // values in flight per CTA

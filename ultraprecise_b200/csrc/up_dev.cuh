@@ -866,6 +866,278 @@ UP_DI void tpi_mul_const(u32 (&r)[K], const u32 (&a)[K], const u32 (&p)[NP]) {
     tpi_window_out<T, K, KA, NP>(r, acc, e);
 }
 
+// Limb `pos` (the same position on every thread of the group; 0 when out of
+// range) broadcast to the whole group.
+template <int T, int K>
+UP_DI u32 tpi_limb(const u32 (&v)[K], int pos) {
+    const bool in = pos >= 0 && pos < T * K;
+    const int src = in ? pos / K : 0;
+    const int li = in ? pos % K : 0;
+    u32 mine = 0u;
+#pragma unroll
+    for (int l = 0; l < K; l++)
+        if (l == li) mine = v[l];
+    const u32 r = __shfl_sync(kFull, mine, src, T);
+    return in ? r : 0u;
+}
+
+// Index of the highest nonzero limb (-1 for zero), on every thread.
+template <int T, int K>
+UP_DI int tpi_top_limb(const u32 (&v)[K]) {
+    int li = -1;
+#pragma unroll
+    for (int i = 0; i < K; i++)
+        if (v[i] != 0u) li = i;
+    const u32 m = tpi_ballot<T>(li >= 0);
+    const int h = m ? 31 - __clz((int)m) : 0;
+    const int top = __shfl_sync(kFull, tpi_rank<T>() * K + li, h, T);
+    return m ? top : -1;
+}
+
+template <int T, int K>
+UP_DI u32 tpi_bitlen(const u32 (&v)[K]) {
+    const int t = tpi_top_limb<T, K>(v);
+    const u32 w = tpi_limb<T, K>(v, t);
+    return t < 0 ? 0u : (u32)(32 * t) + (32u - (u32)__clz((int)w));
+}
+
+// r = v << s bits (0 <= s < 32, the same on every thread; top bits dropped)
+template <int T, int K>
+UP_DI void tpi_shl_bits(u32 (&r)[K], const u32 (&v)[K], u32 s) {
+    u32 below = __shfl_up_sync(kFull, v[K - 1], 1, T);
+    if (tpi_rank<T>() == 0) below = 0u;
+#pragma unroll
+    for (int i = K - 1; i >= 0; i--) {
+        const u32 lo = i > 0 ? v[i - 1] : below;
+        r[i] = s ? ((v[i] << s) | (lo >> (32u - s))) : v[i];
+    }
+}
+
+// r = v >> s bits (0 <= s < 32)
+template <int T, int K>
+UP_DI void tpi_shr_bits(u32 (&r)[K], const u32 (&v)[K], u32 s) {
+    u32 above = __shfl_down_sync(kFull, v[0], 1, T);
+    if (tpi_rank<T>() == T - 1) above = 0u;
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const u32 hi = i < K - 1 ? v[i + 1] : above;
+        r[i] = s ? ((v[i] >> s) | (hi << (32u - s))) : v[i];
+    }
+}
+
+// Long division x = q*b + rem (Knuth's algorithm D) on values spread over the
+// group; b != 0 and x has a zero top limb (room for the normalising shift).
+// The divisor stays in place, normalised so its top bit is set; a window of
+// n+1 remainder limbs aligned with it moves down the dividend one limb per
+// quotient limb.  Each step estimates the quotient limb from three window
+// limbs and two divisor limbs, subtracts quotient x divisor (carry words move
+// up one thread, bit borrows resolve by ballot lookahead), and adds the
+// divisor back when the estimate was one too large.  Groups of a warp may
+// need different step counts: the warp runs the largest, and groups that
+// are done keep their state.
+template <int T, int K>
+UP_DI void tpi_divmod(u32 (&q)[K], u32 (&rem)[K], const u32 (&x)[K], const u32 (&b)[K]) {
+    const int g = tpi_rank<T>();
+    const int n = tpi_top_limb<T, K>(b) + 1;
+    const u32 sh = (u32)__clz((int)tpi_limb<T, K>(b, n - 1));
+    u32 v[K], u[K], R[K];
+    tpi_shl_bits<T, K>(v, b, sh);
+    tpi_shl_bits<T, K>(u, x, sh);
+    const int m = tpi_top_limb<T, K>(u) + 1;
+    const int steps = m >= n ? m - n + 1 : 0;
+    const int j0 = m - n;
+#pragma unroll
+    for (int i = 0; i < K; i++) q[i] = 0u;
+    // window R = u[j0 .. j0+n]; with no steps the remainder is u itself
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int li = ((i + j0) % K + K) % K;
+        u32 mine = 0u;
+#pragma unroll
+        for (int l = 0; l < K; l++)
+            if (l == li) mine = u[l];
+        const int pos = g * K + i + j0;
+        const int src = pos >= 0 && pos < T * K ? pos / K : 0;
+        const u32 w = __shfl_sync(kFull, mine, src, T);
+        R[i] = steps == 0 ? u[i] : ((g * K + i <= n && pos >= 0 && pos < T * K) ? w : 0u);
+    }
+    const u32 vt1 = tpi_limb<T, K>(v, n - 1);
+    const u32 vt2 = tpi_limb<T, K>(v, n - 2);
+    const u32 rcp = reciprocal_u32(vt1);
+    const int S = __reduce_max_sync(kFull, (u32)steps);
+    for (int t = 0; t < S; t++) {
+        const bool active = t < steps;
+        const int j = j0 - t;
+        const u32 r2 = tpi_limb<T, K>(R, n);
+        const u32 r1 = tpi_limb<T, K>(R, n - 1);
+        const u32 r0 = tpi_limb<T, K>(R, n - 2);
+        // quotient limb estimate, at most 2^32-1, refined against vt2
+        u32 qh, rh;
+        bool rh_big = false;
+        if (r2 >= vt1) {
+            qh = 0xffffffffu;
+            const u64 rr = (((u64)r2 << 32) | r1) - (u64)qh * vt1;
+            rh_big = (rr >> 32) != 0;
+            rh = (u32)rr;
+        } else {
+            qh = div2by1(r2, r1, vt1, rcp, rh);
+        }
+#pragma unroll 1
+        for (int c = 0; c < 2; c++) {
+            if (rh_big) break;
+            if ((u64)qh * vt2 <= (((u64)rh << 32) | r0)) break;
+            qh--;
+            const u64 nr = (u64)rh + vt1;
+            rh_big = (nr >> 32) != 0;
+            rh = (u32)nr;
+        }
+        if (!active) qh = 0u;
+        // R -= qh * v: local chains, then carry words up one thread, then bit borrows
+        u32 loc[K];
+        u64 c = 0;
+        u32 br = 0u;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const u64 p = (u64)qh * v[i] + c;
+            c = p >> 32;
+            const u64 d = (u64)R[i] - (u32)p - br;
+            loc[i] = (u32)d;
+            br = (u32)(d >> 63);
+        }
+        const u64 owe = c + br;  // <= 2^32, owed to the next thread's limb 0
+        u32 wlo = __shfl_up_sync(kFull, (u32)owe, 1, T);
+        u32 whi = __shfl_up_sync(kFull, (u32)(owe >> 32), 1, T);
+        if (g == 0) wlo = whi = 0u;
+        u64 win = ((u64)whi << 32) | wlo;
+        u32 any = 0u;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const u64 d = (u64)loc[i] - win;
+            loc[i] = (u32)d;
+            win = (d >> 63) ? 1u : 0u;
+            any |= loc[i];
+        }
+        // bit borrows across threads; a borrow out of the top thread means the
+        // estimate was one too large
+        const u32 G = tpi_ballot<T>(win != 0u);
+        const u32 A = G | tpi_ballot<T>(any == 0u);
+        const u64 sum = (u64)A + G;
+        u32 bin = (u32)(((sum ^ A ^ G) >> g) & 1u);
+        const bool negative = ((sum >> T) & 1u) != 0u;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const u32 t2 = loc[i] - bin;
+            bin = (bin != 0u && loc[i] == 0u) ? 1u : 0u;
+            loc[i] = t2;
+        }
+        // add the divisor back when negative
+        {
+            u64 cc = 0;
+            u32 all = kFull;
+#pragma unroll
+            for (int i = 0; i < K; i++) {
+                cc += (u64)loc[i] + (negative ? v[i] : 0u);
+                loc[i] = (u32)cc;
+                cc >>= 32;
+                all &= loc[i];
+            }
+            tpi_inc_local(loc, tpi_carry_in<T>(cc != 0, all == kFull));
+        }
+        if (negative) qh--;
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < K; i++) R[i] = loc[i];
+            if (j >= 0 && g == j / K) {
+#pragma unroll
+                for (int l = 0; l < K; l++)
+                    if (l == j % K) q[l] = qh;
+            }
+        }
+        // next window: up one limb, u[j-1] enters at the bottom
+        const u32 nxt = tpi_limb<T, K>(u, j - 1);
+        u32 up1 = __shfl_up_sync(kFull, R[K - 1], 1, T);
+        if (active && t + 1 < steps) {
+#pragma unroll
+            for (int i = K - 1; i > 0; i--) R[i] = R[i - 1];
+            R[0] = g == 0 ? nxt : up1;
+        }
+    }
+    tpi_shr_bits<T, K>(rem, R, sh);
+}
+
+// Decimal divide with the rule of div_round (the reference's DivOrMod,
+// AriesDecimal.hxx:748-878) on values spread over the group; LA = limbs of a,
+// p10 = 10^SHIFT (NP limbs), P10W = 10^SHIFT mod 2^64.
+template <int T, int K, int LA, int NP, u32 SHIFT, u64 P10W>
+UP_DI u32 tpi_div_round(u32 (&r)[K], u32& sr, const u32 (&a)[K], u32 sa, const u32 (&b)[K], u32 sb,
+                        const u32 (&p10)[NP]) {
+    const int g = tpi_rank<T>();
+    sr = sa ^ sb;
+    const bool za = tpi_is_zero<T, K>(a);
+    const bool zb = tpi_is_zero<T, K>(b);
+    const u32 hdt = tpi_bitlen<T, K>(a);
+    const u32 hds = tpi_bitlen<T, K>(b);
+    // general path (a zero divisor is replaced by 1 to keep it defined)
+    u32 x[K], bb[K], qv[K], rv[K];
+    tpi_mul_const<T, K, LA, NP>(x, a, p10);
+#pragma unroll
+    for (int i = 0; i < K; i++) bb[i] = zb ? ((g == 0 && i == 0) ? 1u : 0u) : b[i];
+    tpi_divmod<T, K>(qv, rv, x, bb);
+    u32 dbl[K];
+    tpi_add<T, K>(dbl, rv, rv);
+    const bool up_wide = tpi_cmp<T, K>(dbl, bb) >= 0;
+    const u32 rem0 = tpi_limb<T, K>(rv, 0), b0 = tpi_limb<T, K>(bb, 0);
+    const bool up = hds <= 32u ? (u32)(rem0 * 2u) >= b0 : up_wide;
+    {
+        u32 c = (g == 0 && up) ? 1u : 0u, all = kFull;
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const u32 t2 = qv[i] + c;
+            c = (c != 0u && t2 == 0u) ? 1u : 0u;
+            qv[i] = t2;
+            all &= t2;
+        }
+        tpi_inc_local(qv, tpi_carry_in<T>(c != 0u, all == kFull));
+    }
+    // the 64-bit branch
+    const u64 a64 = (u64)tpi_limb<T, K>(a, 0) | ((u64)tpi_limb<T, K>(a, 1) << 32);
+    const u64 b64 = (u64)tpi_limb<T, K>(b, 0) | ((u64)tpi_limb<T, K>(b, 1) << 32);
+    const bool br64 = hdt + ref_shift_bits(SHIFT) - 1u <= 64u && hds <= 64u;
+    u64 q64 = 0;
+    if (br64 && !za && !zb) {
+        const u64 dvs = a64 * P10W;
+        q64 = dvs / b64;
+        const u64 rm = dvs - q64 * b64;
+        q64 += ((rm << 1) >= b64) ? 1u : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int pos = g * K + i;
+        const u32 w64 = pos == 0 ? (u32)q64 : (pos == 1 ? (u32)(q64 >> 32) : 0u);
+        r[i] = za ? 0u : (zb ? a[i] : (br64 ? w64 : qv[i]));
+    }
+    if (za) sr = 0u;
+    return (!za && zb) ? ERR_DIV0 : 0u;
+}
+
+// MOD with the rule of mod (ModCalc): raw magnitudes, scale 0, sign XOR, zero
+// dividend -> +0, zero divisor -> 0 with ERR_DIV0.
+template <int T, int K>
+UP_DI u32 tpi_mod(u32 (&r)[K], u32& sr, const u32 (&a)[K], u32 sa, const u32 (&b)[K], u32 sb) {
+    const int g = tpi_rank<T>();
+    sr = sa ^ sb;
+    const bool za = tpi_is_zero<T, K>(a);
+    const bool zb = tpi_is_zero<T, K>(b);
+    u32 bb[K], qv[K], rv[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) bb[i] = zb ? ((g == 0 && i == 0) ? 1u : 0u) : b[i];
+    tpi_divmod<T, K>(qv, rv, a, bb);
+#pragma unroll
+    for (int i = 0; i < K; i++) r[i] = (za || zb) ? 0u : rv[i];
+    if (za) sr = 0u;
+    return (!za && zb) ? ERR_DIV0 : 0u;
+}
+
 // A distributed copy of a constant held in device memory (nl limbs).
 template <int T, int K>
 UP_DI void tpi_const(u32 (&x)[K], const u32* __restrict__ c, int nl) {
@@ -875,6 +1147,31 @@ UP_DI void tpi_const(u32 (&x)[K], const u32* __restrict__ c, int nl) {
         const int l = g * K + i;
         x[i] = l < nl ? c[l] : 0u;
     }
+}
+
+// Truncation toward zero by 10^d (a RESCALE to a smaller scale); c = the limbs
+// of 10^d in device memory.
+template <int T, int K>
+UP_DI void tpi_trunc_pow10(u32 (&r)[K], const u32 (&a)[K], const u32* __restrict__ c, int nl) {
+    u32 p[K], rv[K];
+    tpi_const<T, K>(p, c, nl);
+    tpi_divmod<T, K>(r, rv, a, p);
+}
+
+// Out-of-line instances of the cooperative wide operations, for expressions
+// that repeat them many times (one instance per operand shape).
+template <int T, int K, int LA, int LB>
+__device__ __noinline__ void tpi_mul_ni(u32 (&r)[K], const u32 (&a)[K], const u32 (&b)[K]) {
+    tpi_mul<T, K, LA, LB>(r, a, b);
+}
+template <int T, int K, int LA, int NP, u32 SHIFT, u64 P10W>
+__device__ __noinline__ u32 tpi_div_round_ni(u32 (&r)[K], u32& sr, const u32 (&a)[K], u32 sa, const u32 (&b)[K],
+                                             u32 sb, const u32 (&p10)[NP]) {
+    return tpi_div_round<T, K, LA, NP, SHIFT, P10W>(r, sr, a, sa, b, sb, p10);
+}
+template <int T, int K>
+__device__ __noinline__ void tpi_trunc_pow10_ni(u32 (&r)[K], const u32 (&a)[K], const u32* __restrict__ c, int nl) {
+    tpi_trunc_pow10<T, K>(r, a, c, nl);
 }
 
 // Compact value of B bytes -> this thread's K limbs and the sign.

@@ -9,6 +9,16 @@ from . import abi, workloads
 from . import expr as E
 
 
+def compile_expr_only(root, cols, threads_per_value: int = 0) -> None:
+    """NVRTC-compile one expression module with the given threads per value."""
+    lib = abi.load()
+    b = E.build([root], cols)
+    E.derive_types(b)
+    opts = abi.UpCompileOpts(threads_per_value, 0, 0)
+    abi.check(lib.up_util_compile_expr_only(b.nodes, b.n_nodes, b.roots[0], b.col_types, b.n_cols, C.byref(opts)),
+              "compile")
+
+
 def _compile(roots, cols, aggs=None):
     lib = abi.load()
     b = E.build(roots, cols)
