@@ -15,16 +15,6 @@ from ultraprecise_b200 import expr as E
 pytestmark = pytest.mark.gpu
 
 
-def _exprs():
-    a, b, c = E.col(0), E.col(1), E.col(2)
-    return {
-        "mad": a * b + c,
-        "msub": a - b * c,
-        "addsub": (a + b) - (c - a),
-        "const": a * E.dec("-12345678901234567890.123") + E.lit(7) * b,
-    }
-
-
 def _columns(p, rows, seed):
     """Edge and random values; every 7th row of column 1 repeats column 0 so
     that sums of opposite signs cancel to +0."""
@@ -52,16 +42,23 @@ def _oracle(e, types, raws, rows):
     return oracle.eval_expr(b, b.roots[0], raws, rows, ob, threads=8)
 
 
-@pytest.mark.parametrize("p", [76, 150, 600])
-@pytest.mark.parametrize("name", ["mad", "msub", "addsub", "const"])
-def test_cooperative_matches_oracle(p, name):
-    s = p // 4
-    e = _exprs()[name]
-    types = [E.ColType(p, s)] * 3
+def _cases(kind):
+    from ultraprecise_b200 import workloads
+    names = {"mul": ("mad", "msub", "addsub", "const"), "div": ("div", "mod", "divmix", "trunc"), "sin": ("sin",)}
+    groups = {}
+    for name, p, e, types, tpv in workloads.coop_cases():
+        if name in names[kind]:
+            groups.setdefault((name, p), (e, types, []))[2].append(tpv)
+    return [(name, p, e, types, tpvs) for (name, p), (e, types, tpvs) in sorted(groups.items(),
+                                                                            key=lambda x: (x[0][1], x[0][0]))]
+
+
+@pytest.mark.parametrize("name,p,e,types,tpvs", _cases("mul"), ids=lambda x: str(x)[:12])
+def test_cooperative_matches_oracle(name, p, e, types, tpvs):
     rows = 3001
     raws = [codec.encode(v, p) for v in _columns(p, rows, seed=p * 31 + len(name))]
     exp, exp_err = _oracle(e, types, raws, rows)
-    for tpv in (0, 2, 8, 32):
+    for tpv in tpvs:
         got, err = _run(e, types, raws, rows, tpv)
         assert got == exp, f"threads_per_value={tpv}"
         assert err == exp_err
@@ -95,44 +92,32 @@ def test_automatic_choice_of_cooperative_path():
         assert ("up_trow" in src) == coop, p
 
 
-def _div_exprs():
-    a, b, c = E.col(0), E.col(1), E.col(2)
-    return {"div": a / b, "mod": a % b, "divmix": (a * c) / b + a, "trunc": E.rescale(a * b, 0, 1)}
-
-
-@pytest.mark.parametrize("p", [38, 150, 300])
-@pytest.mark.parametrize("name", ["div", "mod", "divmix", "trunc"])
-def test_cooperative_division_matches_oracle(p, name):
+@pytest.mark.parametrize("name,p,e,types,tpvs", _cases("div"), ids=lambda x: str(x)[:12])
+def test_cooperative_division_matches_oracle(name, p, e, types, tpvs):
     """Division in every branch of the divide rule: zero dividends and
     divisors (edge values include zeros), small operands (the 64-bit branch),
     one-limb divisors (remainder doubled mod 2^32), and wide divisors."""
-    s = p // 4
-    e = _div_exprs()[name]
-    if name == "trunc":
-        e = E.rescale(E.col(0) * E.col(1), 2 * p + 1, s)  # scale 2s -> s: truncation by 10^s
-    types = [E.ColType(p, s)] * 3
     rows = 3001
-    rng = random.Random(p + len(name))
     vals = _columns(p, rows, seed=p * 7 + len(name))
     # small values on some rows: one-limb divisors and the 64-bit branch
     vals[0] = [(sg, m % 10 ** 12) if i % 5 == 1 else (sg, m) for i, (sg, m) in enumerate(vals[0])]
     vals[1] = [(sg, m % 10 ** 9) if i % 3 == 1 else (sg, m) for i, (sg, m) in enumerate(vals[1])]
     raws = [codec.encode(v, p) for v in vals]
     exp, exp_err = _oracle(e, types, raws, rows)
-    for tpv in (4, 8, 32):
+    for tpv in tpvs:
         got, err = _run(e, types, raws, rows, tpv)
         assert got == exp, f"threads_per_value={tpv}"
         assert err == exp_err
 
 
-@pytest.mark.parametrize("p,rows,tpv", [(100, 3000, 8), (300, 1500, 16), (1000, 300, 32)])
-def test_cooperative_sin_matches_oracle(p, rows, tpv):
+@pytest.mark.parametrize("name,p,e,types,tpvs", _cases("sin"), ids=lambda x: str(x)[:12])
+def test_cooperative_sin_matches_oracle(name, p, e, types, tpvs):
     from ultraprecise_b200 import workloads
-    s = p - 2
-    pi = workloads.pi_scaled(s)
+    rows = 1500
+    pi = workloads.pi_scaled(p - 2)
     raw = codec.encode([(0, 0), (1, 0), (0, pi), (1, pi), (0, 1)], p) + workloads.sin_inputs(p, rows - 5, seed=p)
-    e, cols = workloads.sin_expr(p)
-    exp, exp_err = _oracle(e, cols, [raw], rows)
-    got, err = _run(e, cols, [raw], rows, tpv)
-    assert got == exp
-    assert err == exp_err
+    exp, exp_err = _oracle(e, types, [raw], rows)
+    for tpv in tpvs:
+        got, err = _run(e, types, [raw], rows, tpv)
+        assert got == exp
+        assert err == exp_err

@@ -65,6 +65,11 @@ def prewarm(verbose: bool = False) -> None:
     batch.compile_only(workloads.batch_specs(tasks))
     if verbose:
         print("prewarmed batch module,", len(tasks), "tasks")
+    # the cooperative-evaluation cases of the GPU tests, with their group sizes
+    with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+        list(ex.map(lambda c: compile_expr_only(c[2], c[3], c[4]), workloads.coop_cases()))
+    if verbose:
+        print("prewarmed cooperative cases")
 
 
 def prune(verbose: bool = False) -> None:

@@ -278,3 +278,30 @@ def serve_kinds(n: int, seed: int, mix=SERVE_MIX):
     import random
     rng = random.Random(seed)
     return [rng.choices(range(len(mix)), weights=mix)[0] for _ in range(n)]
+
+
+# Cooperative-evaluation parity cases (the GPU tests run them; the prewarm
+# compiles them): (name, p, expression, column types, threads per value).
+def coop_cases():
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    out = []
+    for p in (76, 150, 600):
+        s = p // 4
+        types = [E.ColType(p, s)] * 3
+        exprs = {"mad": a * b + c, "msub": a - b * c, "addsub": (a + b) - (c - a),
+                 "const": a * E.dec("-12345678901234567890.123") + E.lit(7) * b}
+        for name, e in exprs.items():
+            for tpv in (0, 2, 8, 32):
+                out.append((name, p, e, types, tpv))
+    for p in (38, 150, 300):
+        s = p // 4
+        types = [E.ColType(p, s)] * 3
+        exprs = {"div": a / b, "mod": a % b, "divmix": (a * c) / b + a,
+                 "trunc": E.rescale(a * b, 2 * p + 1, s)}
+        for name, e in exprs.items():
+            for tpv in (4, 8, 32):
+                out.append((name, p, e, types, tpv))
+    for p, tpv in ((100, 8), (300, 16)):
+        e, types = sin_expr(p)
+        out.append(("sin", p, e, types, tpv))
+    return out
