@@ -150,8 +150,9 @@ def build_expr(case):
 
 # DRAM bytes per row (dram__bytes_read.sum + dram__bytes_write.sum of one ncu
 # capture, divided by the rows of the captured launch) for the sweep cases
-# profiled so far: profiles/up_expr_tile_p600_mad.md, up_expr_tile_p38_mad.md.
-NCU_TRAFFIC_PER_ROW = {(600, "mad"): 334.6e6 / 262144, (38, "mad"): 301.58e6 / 4194304}
+# profiled so far: profiles/up_expr_tile_p600_mad_cooperative.md,
+# up_expr_tile_p38_mad.md.
+NCU_TRAFFIC_PER_ROW = {(600, "mad"): (196.66e6 + 96.51e6) / 262144, (38, "mad"): 301.58e6 / 4194304}
 
 
 # ---------------------------------------------------------- our arm

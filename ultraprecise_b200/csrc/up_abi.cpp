@@ -315,6 +315,8 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
                                                                   : "up_query_tile_g";
             a.vec_ok = (vec_ok && aligned16(group_ids)) ? 1 : 0;
             void* k = jit_kernel(*m->jm.ks, name);
+            st = set_smem(k, g.q_smem);  // the tile layout is kept within 48 KB: normally a no-op
+            if (st != UP_OK) return st;
             const int64_t ntiles = (rows + g.q_tile_rows - 1) / g.q_tile_rows;
             // the register and shared-memory modes merge once per CTA, so a
             // spread launch keeps a bounded grid of several waves
