@@ -253,6 +253,16 @@ up_status up_query_launch_noalloc(up_module* m, const up_column* in, int32_t n_i
                                   const int32_t* group_ids, int32_t n_groups,
                                   void* const* outs, uint32_t* err_word, void* stream);
 
+/* Launch over columns in HOST memory (page-locked for full speed): the rows
+ * are cut into chunks whose inputs are copied in, computed and copied back
+ * out on three streams, so copies in, kernels and copies out of successive
+ * chunks overlap.  Contiguous non-null columns (up_column.data is the host
+ * pointer); host_out receives rows * value_bytes.  chunk_rows 0 = about 64 MB
+ * of input per chunk.  Returns when host_out holds every row; *err_word
+ * (host, may be NULL) receives the OR of the row errors. */
+up_status up_expr_launch_host(up_module* m, const up_column* host_in, int32_t n_in, int64_t rows,
+                              void* host_out, uint32_t* err_word, int64_t chunk_rows);
+
 /* ------------------------------------------------------------ utilities */
 /* Measured device facts used by the roofline report. */
 typedef struct up_device_info {

@@ -133,3 +133,22 @@ def test_module_cache_reuses_kernels():
     m2 = runtime.compile_expr(E.col(0) + E.col(1), cols)
     assert lib.up_module_cache_size(0) == n1
     assert m1.source() == m2.source()
+
+
+@pytest.mark.parametrize("p,op,rows,chunk", [(18, "mad", 100_003, 0), (38, "div", 50_001, 7_000),
+                                             (150, "mad", 20_000, 3_001), (600, "mad", 5_000, 999)])
+def test_host_launch_matches_device_launch(p, op, rows, chunk):
+    """up_expr_launch_host (host columns, chunked and overlapped) gives the
+    same bytes and error word as the device launch."""
+    from ultraprecise_b200 import workloads
+    e, cols = workloads.sweep_expr(p, op)
+    m = runtime.compile_expr(e, cols)
+    dev = [runtime.gen_digits(rows, p, 300 + k, nonzero=(op == "div" and k == 1)) for k in range(len(cols))]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    want = m.launch([runtime.DeviceColumn(d, p, p // 4) for d in dev], rows, err=err)
+    torch.cuda.synchronize()
+    host = [d.cpu().pin_memory() if i % 2 == 0 else d.cpu() for i, d in enumerate(dev)]  # pinned and pageable
+    out = torch.empty(rows * m.value_bytes, dtype=torch.uint8).pin_memory()
+    herr = m.launch_host(host, cols, rows, out, chunk_rows=chunk)
+    assert bytes(out.numpy().tobytes()) == bytes(want.cpu().numpy().tobytes())
+    assert herr == int(err.item())

@@ -246,6 +246,110 @@ up_status expr_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_
 extern "C" {
 
 
+up_status up_expr_launch_host(up_module* m, const up_column* host_in, int32_t n_in, int64_t rows, void* host_out,
+                              uint32_t* err_word, int64_t chunk_rows) {
+    if (!m || m->is_query) return fail(UP_ERR_INVALID_ARG, "not an expression module");
+    if (rows < 0 || chunk_rows < 0) return fail(UP_ERR_INVALID_ARG, "negative size");
+    if (err_word) *err_word = 0u;
+    if (rows == 0) return UP_OK;
+    if (!host_out || (n_in > 0 && !host_in)) return fail(UP_ERR_INVALID_ARG, "NULL buffers");
+    const GeneratedModule& g = m->jm.gen;
+    const int nc = (int)g.in_bytes.size();
+    if (n_in < nc) return fail(UP_ERR_INVALID_ARG, "fewer input columns than compiled");
+    int64_t in_row = 0;
+    for (int c = 0; c < nc; c++) {
+        const up_column& col = host_in[c];
+        if (!col.data || col.n_blocks > 0 || col.indices || col.nullable || col.value_bytes != g.in_bytes[c])
+            return fail(UP_ERR_INVALID_ARG, "host launch takes contiguous non-null columns of the compiled width");
+        in_row += col.value_bytes;
+    }
+    const int64_t out_row = g.out_bytes;
+    if (chunk_rows == 0) chunk_rows = std::max<int64_t>(4096, ((int64_t)64 << 20) / std::max<int64_t>(in_row, 1));
+    chunk_rows = std::max<int64_t>(1, std::min(chunk_rows, rows));
+    constexpr int NB = 3;  // buffer sets in rotation
+    const int64_t nchunks = (rows + chunk_rows - 1) / chunk_rows;
+    cudaStream_t s_in = nullptr, s_k = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[NB] = {}, ev_k[NB] = {}, ev_out[NB] = {};
+    void* dev = nullptr;
+    uint32_t* derr = nullptr;
+    up_status st = UP_OK;
+    cudaError_t e = cudaSuccess;
+    // one allocation: NB x (every input column + the output) + the error word
+    std::vector<int64_t> col_off(nc);
+    int64_t set_bytes = 0;
+    for (int c = 0; c < nc; c++) {
+        col_off[c] = set_bytes;
+        set_bytes += (chunk_rows * g.in_bytes[c] + 255) / 256 * 256;
+    }
+    const int64_t out_off = set_bytes;
+    set_bytes += (chunk_rows * out_row + 255) / 256 * 256;
+    auto cleanup = [&]() {
+        if (s_out) cudaStreamSynchronize(s_out);
+        if (s_k) cudaStreamSynchronize(s_k);
+        if (s_in) cudaStreamSynchronize(s_in);
+        if (dev) cudaFree(dev);
+        for (int i = 0; i < NB; i++) {
+            if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+            if (ev_k[i]) cudaEventDestroy(ev_k[i]);
+            if (ev_out[i]) cudaEventDestroy(ev_out[i]);
+        }
+        if (s_in) cudaStreamDestroy(s_in);
+        if (s_k) cudaStreamDestroy(s_k);
+        if (s_out) cudaStreamDestroy(s_out);
+    };
+    e = cudaMalloc(&dev, (size_t)(NB * set_bytes + 256));
+    for (cudaStream_t* sp : {&s_in, &s_k, &s_out})
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking);
+    for (int i = 0; i < NB && e == cudaSuccess; i++) {
+        e = cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_k[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) {
+        derr = (uint32_t*)((uint8_t*)dev + NB * set_bytes);
+        e = cudaMemsetAsync(derr, 0, 4, s_k);
+    }
+    std::vector<up_column> dcol(host_in, host_in + n_in);
+    for (int64_t ch = 0; ch < nchunks && e == cudaSuccess && st == UP_OK; ch++) {
+        const int b = (int)(ch % NB);
+        const int64_t r0 = ch * chunk_rows;
+        const int64_t nr = std::min(chunk_rows, rows - r0);
+        uint8_t* base = (uint8_t*)dev + b * set_bytes;
+        // inputs: this buffer set is free once the kernel of chunk ch-NB has run
+        if (ch >= NB) e = cudaStreamWaitEvent(s_in, ev_k[b], 0);
+        for (int c = 0; c < nc && e == cudaSuccess; c++) {
+            const int64_t w = g.in_bytes[c];
+            e = cudaMemcpyAsync(base + col_off[c], (const uint8_t*)host_in[c].data + r0 * w, (size_t)(nr * w),
+                                cudaMemcpyHostToDevice, s_in);
+            dcol[c].data = base + col_off[c];
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev_in[b], s_in);
+        // kernel: after its inputs landed and the copy-out of chunk ch-NB left the output buffer
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s_k, ev_in[b], 0);
+        if (e == cudaSuccess && ch >= NB) e = cudaStreamWaitEvent(s_k, ev_out[b], 0);
+        if (e == cudaSuccess) st = expr_launch_ex(m, dcol.data(), n_in, nr, base + out_off, derr, s_k, false);
+        if (e == cudaSuccess && st == UP_OK) e = cudaEventRecord(ev_k[b], s_k);
+        // outputs
+        if (e == cudaSuccess && st == UP_OK) e = cudaStreamWaitEvent(s_out, ev_k[b], 0);
+        if (e == cudaSuccess && st == UP_OK)
+            e = cudaMemcpyAsync((uint8_t*)host_out + r0 * out_row, base + out_off, (size_t)(nr * out_row),
+                                cudaMemcpyDeviceToHost, s_out);
+        if (e == cudaSuccess && st == UP_OK) e = cudaEventRecord(ev_out[b], s_out);
+    }
+    uint32_t herr = 0;
+    if (e == cudaSuccess && st == UP_OK) {
+        e = cudaStreamWaitEvent(s_out, ev_k[(nchunks - 1) % NB], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s_out);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s_out);
+    }
+    const cudaError_t e_final = e;
+    cleanup();
+    if (st != UP_OK) return st;
+    if (e_final != cudaSuccess) return cuda_fail(e_final, "host launch");
+    if (err_word) *err_word = herr;
+    return UP_OK;
+}
+
 up_status up_query_compile(const up_expr_node* nodes, int32_t n_nodes, const up_col_type* cols, int32_t n_cols,
                            const up_query_agg* aggs, int32_t n_aggs, const up_compile_opts* opts, up_module** out) {
     if (!out) return fail(UP_ERR_INVALID_ARG, "out is NULL");

@@ -106,6 +106,24 @@ class ExprModule:
                   "up_expr_launch")
         return out
 
+    def launch_host(self, cols: Sequence[torch.Tensor], types: Sequence[ColType], rows: int, out: torch.Tensor,
+                    chunk_rows: int = 0) -> int:
+        """Launch over HOST columns (uint8 CPU tensors, ideally pinned): the
+        rows stream through the GPU in overlapped chunks; `out` (uint8 CPU
+        tensor of rows*value_bytes) receives the results.  Returns the OR of
+        the row errors."""
+        lib = abi.load()
+        arr = (abi.UpColumn * max(1, len(cols)))()
+        for i, (t, ct) in enumerate(zip(cols, types)):
+            arr[i].data = t.data_ptr()
+            arr[i].precision = ct.precision
+            arr[i].scale = ct.scale
+            arr[i].value_bytes = codec.compact_bytes(ct.precision)
+        err = C.c_uint32(0)
+        abi.check(lib.up_expr_launch_host(self._h, arr, len(cols), rows, out.data_ptr(), C.byref(err), chunk_rows),
+                  "up_expr_launch_host")
+        return err.value
+
     def __del__(self):
         try:
             abi.load().up_module_release(self._h)
