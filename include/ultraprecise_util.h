@@ -52,6 +52,11 @@ up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32
 up_status up_util_compile_expr_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
                                     const up_col_type* cols, int32_t n_cols, const up_compile_opts* opts);
 
+/* Generated CUDA source of an expression module (no compile, no GPU):
+ * returns its length; copies at most cap-1 bytes + NUL when buf != NULL. */
+int64_t up_util_expr_source(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
+                            int32_t n_cols, const up_compile_opts* opts, char* buf, int64_t cap);
+
 struct up_batch_task;
 up_status up_util_compile_batch_only(const struct up_batch_task* tasks, int32_t n_tasks);
 

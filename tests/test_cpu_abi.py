@@ -102,3 +102,18 @@ def test_launch_without_device_fails_loudly():
     lib = abi.load()
     info = abi.UpDeviceInfo()
     assert lib.up_device_query(0, C.byref(info)) != abi.UP_OK
+
+
+def test_automatic_choice_of_cooperative_path():
+    """The widest a*b+c sweep expression gets the cooperative kernel (16
+    threads per value), narrower ones and divisions one thread per value;
+    threads_per_value overrides the choice."""
+    from ultraprecise_b200 import prewarm, workloads
+    for p, op, coop in ((150, "mad", False), (300, "mad", False), (600, "mad", True), (600, "div", False)):
+        e, cols = workloads.sweep_expr(p, op)
+        src = prewarm.expr_source(e, cols)
+        assert ("up_trow" in src) == coop, (p, op)
+    e, cols = workloads.sweep_expr(600, "mad")
+    assert "tpi_mul<16, 8" in prewarm.expr_source(e, cols)
+    assert "up_trow" not in prewarm.expr_source(e, cols, threads_per_value=1)
+    assert "tpi_div_round<8," in prewarm.expr_source(*workloads.sweep_expr(150, "div"), threads_per_value=8)

@@ -82,14 +82,6 @@ def test_cooperative_products_rescale_compare(p):
             assert got == exp and err == exp_err, f"threads_per_value={tpv}"
 
 
-def test_automatic_choice_of_cooperative_path():
-    """The widest a*b+c sweep expression compiles to the cooperative kernel,
-    narrower ones to one thread per value."""
-    from ultraprecise_b200 import workloads
-    for p, coop in ((150, False), (300, False), (600, True)):
-        e, cols = workloads.sweep_expr(p, "mad")
-        src = runtime.compile_expr(e, cols).source()
-        assert ("up_trow" in src) == coop, p
 
 
 @pytest.mark.parametrize("name,p,e,types,tpvs", _cases("div"), ids=lambda x: str(x)[:12])

@@ -14,6 +14,7 @@ SIGNATURES = {
     "up_util_imad_peak": (_I32, [C.POINTER(C.c_double), _P]),
     "up_util_compile_only": (_I32, [_P, _I32, _I32, _P, _I32, _I32, _P, _I32]),
     "up_util_compile_expr_only": (_I32, [_P, _I32, _I32, _P, _I32, _P]),
+    "up_util_expr_source": (_I64, [_P, _I32, _I32, _P, _I32, _P, C.c_char_p, _I64]),
     # ultraprecise_batch.h
     "up_batch_create": (_I32, [_P, _I32, _P, C.POINTER(_P)]),
     "up_batch_bind": (_I32, [_P, _I32, _P, _I32, _I64, _P, _I32, _P]),

@@ -544,6 +544,19 @@ up_status up_util_compile_expr_only(const up_expr_node* nodes, int32_t n_nodes, 
     return jit_compile_cubin(gen.source, cubin);
 }
 
+int64_t up_util_expr_source(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
+                            int32_t n_cols, const up_compile_opts* opts, char* buf, int64_t cap) {
+    GeneratedModule gen;
+    if (generate_expr_module(nodes, n_nodes, root, cols, n_cols, opts, gen) != UP_OK) return -1;
+    const int64_t n = (int64_t)gen.source.size();
+    if (buf && cap > 0) {
+        const int64_t k = std::min(n, cap - 1);
+        memcpy(buf, gen.source.data(), (size_t)k);
+        buf[k] = '\0';
+    }
+    return n;
+}
+
 up_status up_device_query(int32_t device, up_device_info* info) {
     if (!info) return fail(UP_ERR_INVALID_ARG, "info is NULL");
     memset(info, 0, sizeof *info);

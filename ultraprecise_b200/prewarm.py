@@ -19,6 +19,20 @@ def compile_expr_only(root, cols, threads_per_value: int = 0) -> None:
               "compile")
 
 
+def expr_source(root, cols, threads_per_value: int = 0) -> str:
+    """Generated CUDA source of an expression module (CPU only)."""
+    lib = abi.load()
+    b = E.build([root], cols)
+    E.derive_types(b)
+    opts = abi.UpCompileOpts(threads_per_value, 0, 0)
+    n = lib.up_util_expr_source(b.nodes, b.n_nodes, b.roots[0], b.col_types, b.n_cols, C.byref(opts), None, 0)
+    if n < 0:
+        raise ValueError("expression rejected")
+    buf = C.create_string_buffer(int(n) + 1)
+    lib.up_util_expr_source(b.nodes, b.n_nodes, b.roots[0], b.col_types, b.n_cols, C.byref(opts), buf, n + 1)
+    return buf.value.decode()
+
+
 def _compile(roots, cols, aggs=None):
     lib = abi.load()
     b = E.build(roots, cols)
