@@ -266,15 +266,9 @@ up_status up_expr_launch_host(up_module* m, const up_column* host_in, int32_t n_
     const int64_t out_row = g.out_bytes;
     if (chunk_rows == 0) chunk_rows = std::max<int64_t>(4096, ((int64_t)64 << 20) / std::max<int64_t>(in_row, 1));
     chunk_rows = std::max<int64_t>(1, std::min(chunk_rows, rows));
-    constexpr int NB = 3;  // buffer sets in rotation
+    constexpr int NB = HostStaging::kSets;
     const int64_t nchunks = (rows + chunk_rows - 1) / chunk_rows;
-    cudaStream_t s_in = nullptr, s_k = nullptr, s_out = nullptr;
-    cudaEvent_t ev_in[NB] = {}, ev_k[NB] = {}, ev_out[NB] = {};
-    void* dev = nullptr;
-    uint32_t* derr = nullptr;
-    up_status st = UP_OK;
-    cudaError_t e = cudaSuccess;
-    // one allocation: NB x (every input column + the output) + the error word
+    // one buffer set: every input column + the output, 256-byte aligned
     std::vector<int64_t> col_off(nc);
     int64_t set_bytes = 0;
     for (int c = 0; c < nc; c++) {
@@ -283,69 +277,54 @@ up_status up_expr_launch_host(up_module* m, const up_column* host_in, int32_t n_
     }
     const int64_t out_off = set_bytes;
     set_bytes += (chunk_rows * out_row + 255) / 256 * 256;
-    auto cleanup = [&]() {
-        if (s_out) cudaStreamSynchronize(s_out);
-        if (s_k) cudaStreamSynchronize(s_k);
-        if (s_in) cudaStreamSynchronize(s_in);
-        if (dev) cudaFree(dev);
-        for (int i = 0; i < NB; i++) {
-            if (ev_in[i]) cudaEventDestroy(ev_in[i]);
-            if (ev_k[i]) cudaEventDestroy(ev_k[i]);
-            if (ev_out[i]) cudaEventDestroy(ev_out[i]);
-        }
-        if (s_in) cudaStreamDestroy(s_in);
-        if (s_k) cudaStreamDestroy(s_k);
-        if (s_out) cudaStreamDestroy(s_out);
-    };
-    e = cudaMalloc(&dev, (size_t)(NB * set_bytes + 256));
-    for (cudaStream_t* sp : {&s_in, &s_k, &s_out})
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking);
-    for (int i = 0; i < NB && e == cudaSuccess; i++) {
-        e = cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_k[i], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming);
-    }
-    if (e == cudaSuccess) {
-        derr = (uint32_t*)((uint8_t*)dev + NB * set_bytes);
-        e = cudaMemsetAsync(derr, 0, 4, s_k);
-    }
+    // the module keeps its staging buffers, streams and events between calls
+    std::lock_guard<std::mutex> lk(m->host_mu);
+    HostStaging& hs = m->host;
+    up_status st = hs.ensure((size_t)(NB * set_bytes + 256));
+    if (st != UP_OK) return st;
+    cudaError_t e = cudaSuccess;
+    uint32_t* derr = (uint32_t*)((uint8_t*)hs.dev + NB * set_bytes);
+    e = cudaMemsetAsync(derr, 0, 4, hs.s_k);
+    // the previous call finished (it synchronised), so every buffer set is free
     std::vector<up_column> dcol(host_in, host_in + n_in);
     for (int64_t ch = 0; ch < nchunks && e == cudaSuccess && st == UP_OK; ch++) {
         const int b = (int)(ch % NB);
         const int64_t r0 = ch * chunk_rows;
         const int64_t nr = std::min(chunk_rows, rows - r0);
-        uint8_t* base = (uint8_t*)dev + b * set_bytes;
+        uint8_t* base = (uint8_t*)hs.dev + b * set_bytes;
         // inputs: this buffer set is free once the kernel of chunk ch-NB has run
-        if (ch >= NB) e = cudaStreamWaitEvent(s_in, ev_k[b], 0);
+        if (ch >= NB) e = cudaStreamWaitEvent(hs.s_in, hs.ev_k[b], 0);
         for (int c = 0; c < nc && e == cudaSuccess; c++) {
             const int64_t w = g.in_bytes[c];
             e = cudaMemcpyAsync(base + col_off[c], (const uint8_t*)host_in[c].data + r0 * w, (size_t)(nr * w),
-                                cudaMemcpyHostToDevice, s_in);
+                                cudaMemcpyHostToDevice, hs.s_in);
             dcol[c].data = base + col_off[c];
         }
-        if (e == cudaSuccess) e = cudaEventRecord(ev_in[b], s_in);
+        if (e == cudaSuccess) e = cudaEventRecord(hs.ev_in[b], hs.s_in);
         // kernel: after its inputs landed and the copy-out of chunk ch-NB left the output buffer
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s_k, ev_in[b], 0);
-        if (e == cudaSuccess && ch >= NB) e = cudaStreamWaitEvent(s_k, ev_out[b], 0);
-        if (e == cudaSuccess) st = expr_launch_ex(m, dcol.data(), n_in, nr, base + out_off, derr, s_k, false);
-        if (e == cudaSuccess && st == UP_OK) e = cudaEventRecord(ev_k[b], s_k);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(hs.s_k, hs.ev_in[b], 0);
+        if (e == cudaSuccess && ch >= NB) e = cudaStreamWaitEvent(hs.s_k, hs.ev_out[b], 0);
+        if (e == cudaSuccess) st = expr_launch_ex(m, dcol.data(), n_in, nr, base + out_off, derr, hs.s_k, false);
+        if (e == cudaSuccess && st == UP_OK) e = cudaEventRecord(hs.ev_k[b], hs.s_k);
         // outputs
-        if (e == cudaSuccess && st == UP_OK) e = cudaStreamWaitEvent(s_out, ev_k[b], 0);
+        if (e == cudaSuccess && st == UP_OK) e = cudaStreamWaitEvent(hs.s_out, hs.ev_k[b], 0);
         if (e == cudaSuccess && st == UP_OK)
             e = cudaMemcpyAsync((uint8_t*)host_out + r0 * out_row, base + out_off, (size_t)(nr * out_row),
-                                cudaMemcpyDeviceToHost, s_out);
-        if (e == cudaSuccess && st == UP_OK) e = cudaEventRecord(ev_out[b], s_out);
+                                cudaMemcpyDeviceToHost, hs.s_out);
+        if (e == cudaSuccess && st == UP_OK) e = cudaEventRecord(hs.ev_out[b], hs.s_out);
     }
     uint32_t herr = 0;
     if (e == cudaSuccess && st == UP_OK) {
-        e = cudaStreamWaitEvent(s_out, ev_k[(nchunks - 1) % NB], 0);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s_out);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s_out);
+        e = cudaStreamWaitEvent(hs.s_out, hs.ev_k[(nchunks - 1) % NB], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, hs.s_out);
     }
-    const cudaError_t e_final = e;
-    cleanup();
+    // always leave the staging idle before returning
+    const cudaError_t e1 = cudaStreamSynchronize(hs.s_out);
+    const cudaError_t e2 = cudaStreamSynchronize(hs.s_k);
+    const cudaError_t e3 = cudaStreamSynchronize(hs.s_in);
     if (st != UP_OK) return st;
-    if (e_final != cudaSuccess) return cuda_fail(e_final, "host launch");
+    for (cudaError_t x : {e, e1, e2, e3})
+        if (x != cudaSuccess) return cuda_fail(x, "host launch");
     if (err_word) *err_word = herr;
     return UP_OK;
 }

@@ -3,8 +3,11 @@
 #ifndef UP_INTERNAL_H_
 #define UP_INTERNAL_H_
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -130,9 +133,55 @@ void mkdir_if_missing(const std::string& dir);
 
 }  // namespace upi
 
+// Device staging of up_expr_launch_host, kept by the module between calls:
+// kSets buffer sets in rotation, the three streams and their events.
+struct HostStaging {
+    static constexpr int kSets = 3;
+    void* dev = nullptr;
+    size_t bytes = 0;
+    cudaStream_t s_in = nullptr, s_k = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[kSets] = {}, ev_k[kSets] = {}, ev_out[kSets] = {};
+    up_status ensure(size_t need) {
+        if (!s_in) {
+            for (cudaStream_t* sp : {&s_in, &s_k, &s_out})
+                if (cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking) != cudaSuccess) return bad();
+            for (int i = 0; i < kSets; i++)
+                for (cudaEvent_t* ep : {&ev_in[i], &ev_k[i], &ev_out[i]})
+                    if (cudaEventCreateWithFlags(ep, cudaEventDisableTiming) != cudaSuccess) return bad();
+        }
+        if (need > bytes) {
+            if (dev) cudaFree(dev);
+            dev = nullptr;
+            bytes = 0;
+            if (cudaMalloc(&dev, need) != cudaSuccess) {
+                cudaGetLastError();
+                return upi::fail(UP_ERR_NO_MEMORY, "host launch staging");
+            }
+            bytes = need;
+        }
+        return UP_OK;
+    }
+    up_status bad() {
+        cudaGetLastError();
+        return upi::fail(UP_ERR_CUDA, "host launch streams");
+    }
+    ~HostStaging() {
+        for (cudaStream_t s : {s_in, s_k, s_out})
+            if (s) cudaStreamSynchronize(s);
+        if (dev) cudaFree(dev);
+        for (int i = 0; i < kSets; i++)
+            for (cudaEvent_t ev : {ev_in[i], ev_k[i], ev_out[i]})
+                if (ev) cudaEventDestroy(ev);
+        for (cudaStream_t s : {s_in, s_k, s_out})
+            if (s) cudaStreamDestroy(s);
+    }
+};
+
 struct up_module {
     upi::JitModule jm;
     bool is_query = false;
+    std::mutex host_mu;   // one host launch at a time per module
+    HostStaging host;
 };
 
 // Launch variants used by the serving loop: `spread` launches one CTA per
