@@ -883,8 +883,12 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     int R = 1024;
     while (R > 128 && 2L * R * row_bytes > 32 * 1024) R /= 2;
     const bool staged = 2L * R * row_bytes <= 32 * 1024;
+    // register mode keeps per group a count and, per accumulator, its full
+    // width when that is at most 4 limbs, else a 128-bit fast accumulator
+    int reg_words = 1;
+    for (int n : acc_limbs) reg_words += std::min(n, 4);
     int GR = 0;
-    while (GR < 8 && (GR + 1) * (accw + 1) <= 96) GR++;
+    while (GR < 8 && (GR + 1) * reg_words <= 96) GR++;
     out.q_staged = staged;
     out.q_tile_rows = R;
     out.q_gr = GR;
@@ -920,12 +924,16 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         src << "    const int nsm = MODE == 0 ? (ng < GR ? ng : GR) : (MODE == 1 ? ng : 0);\n";
         src << "    for (int i = threadIdx.x; i < nsm * W; i += blockDim.x) sacc[i] = 0u;\n";
         src << "    for (int i = threadIdx.x; i < nsm; i += blockDim.x) scnt[i] = 0u;\n";
+        // register accumulators: the full width when it is at most 4 limbs, else a
+        // 128-bit fast accumulator for values that fit 64 bits (the others go
+        // straight to the shared-memory accumulators)
+        auto ra_limbs = [&](int i) { return acc_limbs[i] <= 4 ? acc_limbs[i] : 4; };
         for (int i = 0; i < NR; i++)
-            src << "    u32 ra" << i << "[MODE == 0 ? GR : 1][" << acc_limbs[i] << "];\n";
+            src << "    u32 ra" << i << "[MODE == 0 ? GR : 1][" << ra_limbs(i) << "];\n";
         src << "    u32 rc[MODE == 0 ? GR : 1];\n";
         src << "#pragma unroll\n    for (int j = 0; j < (MODE == 0 ? GR : 1); j++) {\n        rc[j] = 0u;\n";
         for (int i = 0; i < NR; i++)
-            src << "#pragma unroll\n        for (int l = 0; l < " << acc_limbs[i] << "; l++) ra" << i << "[j][l] = 0u;\n";
+            src << "#pragma unroll\n        for (int l = 0; l < " << ra_limbs(i) << "; l++) ra" << i << "[j][l] = 0u;\n";
         src << "    }\n";
         src << "    const i64 ntiles = (a.rows + R - 1) / R;\n";
         src << "    const i64 nfull = a.vec_ok ? a.rows / R : 0;  // tiles moved by bulk copies\n";
@@ -979,9 +987,20 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
             src << "true" << targs() << ");\n";
         }
         src << "            if constexpr (MODE == 0) {\n";
+        for (int i = 0; i < NR; i++)
+            if (acc_limbs[i] > 4) {
+                src << "                const bool f" << i << " = fits_twos64(qv" << i << ");\n";
+                src << "                if (!f" << i << ") atomic_add_twos(sacc + g * W + " << acc_off[i] << ", qv" << i
+                    << ");  // rare: wider than 64 bits\n";
+            }
         src << "#pragma unroll\n                for (int j = 0; j < GR; j++)\n";
         src << "                    if (g == j) {\n                        rc[j]++;\n";
-        for (int i = 0; i < NR; i++) src << "                        add_twos(ra" << i << "[j], qv" << i << ");\n";
+        for (int i = 0; i < NR; i++) {
+            if (acc_limbs[i] > 4)
+                src << "                        if (f" << i << ") add_twos64(ra" << i << "[j], qv" << i << ");\n";
+            else
+                src << "                        add_twos(ra" << i << "[j], qv" << i << ");\n";
+        }
         src << "                    }\n";
         src << "            } else if constexpr (MODE == 1) {\n";
         src << "                atomicAdd(scnt + g, 1u);\n";
@@ -1003,8 +1022,16 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         src << "#pragma unroll\n        for (int j = 0; j < GR; j++)\n";
         src << "            if (rc[j] != 0u) {\n";
         src << "                atomicAdd(scnt + j, rc[j]);\n";
-        for (int i = 0; i < NR; i++)
-            src << "                atomic_add_twos(sacc + j * W + " << acc_off[i] << ", ra" << i << "[j]);\n";
+        for (int i = 0; i < NR; i++) {
+            if (acc_limbs[i] > 4) {
+                src << "                {\n                    u32 wide[" << acc_limbs[i] << "];  // sign-extended 128-bit sum\n";
+                src << "#pragma unroll\n                    for (int l = 0; l < " << acc_limbs[i] << "; l++) wide[l] = l < 4 ? ra"
+                    << i << "[j][l < 4 ? l : 0] : ((ra" << i << "[j][3] >> 31) ? 0xffffffffu : 0u);\n";
+                src << "                    atomic_add_twos(sacc + j * W + " << acc_off[i] << ", wide);\n                }\n";
+            } else {
+                src << "                atomic_add_twos(sacc + j * W + " << acc_off[i] << ", ra" << i << "[j]);\n";
+            }
+        }
         src << "            }\n";
         src << "    }\n";
         src << "    if constexpr (MODE != 2) {\n";

@@ -1302,6 +1302,37 @@ UP_DI void atomic_add_twos(u32* acc, const u32 (&t)[NACC]) {
     }
 }
 
+// True when a two's complement value of N limbs equals the sign extension of
+// its low 64 bits.
+template <int N>
+UP_DI bool fits_twos64(const u32 (&t)[N]) {
+    if constexpr (N <= 2) {
+        return true;
+    } else {
+        const u32 ext = (t[1] >> 31) ? 0xffffffffu : 0u;
+        bool f = true;
+#pragma unroll
+        for (int i = 2; i < N; i++) f &= t[i] == ext;
+        return f;
+    }
+}
+
+// 128-bit two's complement accumulator r (4 limbs) += the sign-extended low
+// 64 bits of t.
+template <int N>
+UP_DI void add_twos64(u32 (&r)[4], const u32 (&t)[N]) {
+    const u64 lo = (u64)t[0] | (N > 1 ? ((u64)t[N > 1 ? 1 : 0] << 32) : 0ull);
+    const u64 ext = (N > 1 ? (t[N > 1 ? 1 : 0] >> 31) : (t[0] >> 31)) ? ~0ull : 0ull;
+    const u64 a0 = (u64)r[0] | ((u64)r[1] << 32);
+    const u64 a1 = (u64)r[2] | ((u64)r[3] << 32);
+    const u64 s0 = a0 + lo;
+    const u64 s1 = a1 + ext + (s0 < a0 ? 1ull : 0ull);
+    r[0] = (u32)s0;
+    r[1] = (u32)(s0 >> 32);
+    r[2] = (u32)s1;
+    r[3] = (u32)(s1 >> 32);
+}
+
 // Two's complement image over N limbs of a sign-magnitude value.
 template <int N, int M>
 UP_DI void to_twos(u32 (&t)[N], const u32 (&m)[M], u32 sign) {
