@@ -153,45 +153,9 @@ UP_DI void add_signed(u32 (&r)[N], u32& sr, const u32 (&a)[NA], u32 sa, const u3
     sr = same ? sa : (nz ? (neg ? sb : (sb ^ 1u)) : 0u);
 }
 
-// r = a * b (low N limbs of the product), column by column: limb k of the
-// result is the sum of a[i]*b[k-i], final once written, so operand limbs die
-// as the columns pass them and no partial-result array stays live (fully
-// unrolled sizes).  Each column is summed in four independent chains (low and
-// high product halves, even and odd i), 64-bit each, so consecutive products
-// do not wait on one another: a column of up to 2^20 products stays below 2^52
-// per chain and the carry into the next column below 2^54.
-template <int N, int NA, int NB>
-UP_DI void mul_columns(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
-    u64 carry = 0;
-#pragma unroll
-    for (int k = 0; k < N; k++) {
-        const int i0 = k - (NB - 1) > 0 ? k - (NB - 1) : 0;
-        const int i1 = k < NA - 1 ? k : NA - 1;
-        u64 lo0 = 0, lo1 = 0, hi0 = 0, hi1 = 0;
-#pragma unroll
-        for (int i = i0; i <= i1; i++) {
-            const u64 p = (u64)a[i] * b[k - i];
-            if ((i & 1) == 0) {
-                lo0 += (u32)p;
-                hi0 += p >> 32;
-            } else {
-                lo1 += (u32)p;
-                hi1 += p >> 32;
-            }
-        }
-        const u64 col = lo0 + lo1 + carry;
-        r[k] = (u32)col;
-        carry = (col >> 32) + hi0 + hi1;
-    }
-}
-
 // r = a * b (low N limbs of the product)
 template <int N, int NA, int NB>
 UP_DI void mul(u32 (&r)[N], const u32 (&a)[NA], const u32 (&b)[NB]) {
-    if constexpr (NA * NB <= kMulUnrollPairs && NA > 1 && NB > 1) {
-        mul_columns(r, a, b);
-        return;
-    }
     zero(r);
     // products above UP_MUL_UNROLL_PAIRS limb pairs keep the outer loop rolled
     // (compile time)
@@ -323,6 +287,72 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
     // quotient digits above nx - nb + 1 are zero (x < 2^(32 nx), b >= 2^(32 (nb-1)))
     const int jmax = (int)((bitlen(x) + 31u) >> 5) - (int)((bl + 31u) >> 5) + 1;
     constexpr bool kUnroll = (NX + 1) * NB <= 96;
+    if constexpr (!kUnroll && NB <= 40) {
+        // Wide operands: the rolled loop keeps the current remainder window
+        // un[j .. j+NB] in registers (static indices) and moves it up one limb
+        // per quotient digit, reading a single dividend limb per step, instead
+        // of addressing un[i + j] in local memory 2*NB times per step.  Up to
+        // 40-limb divisors (measured on B200: 1.1x faster at 32 limbs; at 63
+        // limbs window and divisor no longer fit the registers and it is 1.8x
+        // slower).
+#pragma unroll
+        for (int i = 0; i < NX; i++) q[i] = 0u;
+        const int j0 = jmax < NX ? jmax : NX;
+        u32 w[NB + 1];
+#pragma unroll
+        for (int i = 0; i <= NB; i++) w[i] = j0 >= 0 ? un[j0 + i] : 0u;
+#pragma unroll 1
+        for (int j = j0; j >= 0; j--) {
+            const u32 u1 = w[NB], u0 = w[NB - 1];
+            u64 qhat, rhat;
+            if (u1 >= vtop) {
+                qhat = 0xffffffffull;
+                rhat = (u64)u0 + vtop;
+            } else {
+                u32 r32;
+                qhat = div2by1(u1, u0, vtop, vinv, r32);
+                rhat = r32;
+            }
+            while ((rhat >> 32) == 0u && qhat * vnext > ((rhat << 32) | w[NB - 2])) {
+                qhat--;
+                rhat += vtop;
+            }
+            u64 carry = 0;
+            i64 borrow = 0;
+#pragma unroll
+            for (int i = 0; i < NB; i++) {
+                const u64 p = qhat * bn[i] + carry;
+                carry = p >> 32;
+                const i64 t = (i64)w[i] - (i64)(u32)p - borrow;
+                w[i] = (u32)t;
+                borrow = t < 0 ? 1 : 0;
+            }
+            const i64 t = (i64)w[NB] - (i64)carry - borrow;
+            w[NB] = (u32)t;
+            if (t < 0) {
+                qhat--;
+                u64 c = 0;
+#pragma unroll
+                for (int i = 0; i < NB; i++) {
+                    c += (u64)w[i] + bn[i];
+                    w[i] = (u32)c;
+                    c >>= 32;
+                }
+                w[NB] += (u32)c;
+            }
+            if (j < NX) q[j < NX ? j : 0] = (u32)qhat;
+            if (j > 0) {
+#pragma unroll
+                for (int i = NB; i > 0; i--) w[i] = w[i - 1];
+                w[0] = un[j - 1];
+            }
+        }
+        u32 rl[NB];
+#pragma unroll
+        for (int i = 0; i < NB; i++) rl[i] = j0 >= 0 ? w[i] : un[i];
+        shr_bits(rem, rl, s);
+        return;
+    }
 #pragma unroll(kUnroll ? NX + 1 : 1)
     for (int j = NX; j >= 0; j--) {
         if (j > jmax) {

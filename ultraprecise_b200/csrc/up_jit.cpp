@@ -97,11 +97,19 @@ void mkdirs(const std::string& path) {
     }
 }
 
+// The cache key covers everything that decides the CUBIN: target, options,
+// the NVRTC version, the device library header the source includes, and the
+// source itself.
 std::string full_key(const std::string& src, bool rdc) {
     int maj = 0, min = 0;
     nvrtcVersion(&maj, &min);
+    static const std::string hdr_hash = [] {
+        char b[40];
+        snprintf(b, sizeof b, "%016llx", (unsigned long long)fnv1a(device_header_source()));
+        return std::string(b);
+    }();
     return std::string(kArch) + (rdc ? "|rdc" : "") + "|nvrtc" + std::to_string(maj) + "." + std::to_string(min) +
-           "|" + src;
+           "|hdr" + hdr_hash + "|" + src;
 }
 
 bool read_file(const std::string& p, std::string& out) {
