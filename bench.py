@@ -1,7 +1,7 @@
 """Benchmark of the exact-decimal path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sweep|batch|query|sin|serve]
+                    [--workload sweep|batch|query|sin|serve|text]
 
 Workload "sweep" (default) is the precision sweep: element-wise a*b+c and a/b
 (scale s+4, half-up) on DECIMAL(p, p/4), p in {18,38,76,150,300,600}, every
@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query", "sin", "serve"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query", "sin", "serve", "text"])
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per rate (serve workload)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -986,6 +986,59 @@ def run_serve(args, rank, world):
     return res
 
 
+# ------------------------------------------------------------ text workload
+TEXT_METRIC = "decimal rows/s formatted to text and parsed back (DECIMAL(38,9)), bit-exact round trip"
+
+
+def run_text(args, rank, world):
+    """Format 16M DECIMAL(38,9) values to decimal strings and parse the
+    packed strings back (up_format_decimal, up_parse_decimal); a step is both
+    passes, and the parsed column must equal the input."""
+    import torch
+    from ultraprecise_b200 import runtime
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    p, s = 38, 9
+    rows = max(1, int((16 << 20) * args.rows_scale))
+    col = runtime.gen_digits(rows, p, 5 + rank)
+    text, lens = runtime.format_decimal(col, rows, p, s)
+    width = text.shape[1]
+    mask = torch.arange(width, device="cuda")[None, :] < lens[:, None].to(torch.int64)
+    flat = text[mask].contiguous()
+    offsets = torch.zeros(rows + 1, dtype=torch.int64, device="cuda")
+    offsets[1:] = torch.cumsum(lens.to(torch.int64), 0)
+    back, err = runtime.parse_decimal(None, p, s, text=flat, offsets=offsets)
+    ok = err == 0 and bool(torch.equal(back, col))
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+
+    with ClockSampler(dev) as clk:
+        ms_fmt = timed(lambda: runtime.format_decimal(col, rows, p, s))
+        ms_parse = timed(lambda: runtime.parse_decimal(None, p, s, text=flat, offsets=offsets))
+    ms = ms_fmt + ms_parse
+    text_bytes = int(flat.numel())
+    return {"metric": TEXT_METRIC, "value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+            "config": {"workload": f"format + parse {rows} DECIMAL(38,9) values", "round_trip_exact": ok,
+                       "text_bytes": text_bytes, "parallelism": f"replicas x{world}"},
+            "format_ms": round(ms_fmt, 4), "parse_ms": round(ms_parse, 4),
+            "parse_text_gbs": round(text_bytes / (ms_parse * 1e-3) / 1e9, 1),
+            "gpu_launches": 2 * args.steps, "clocks": clk.summary()}
+
+
 # ------------------------------------------------------ CPU baseline
 def cpu_rate(cases, cpu_seconds, threads, seed=1):
     """Time the oracle on the host cores over the same sweep mix (every case
@@ -1032,9 +1085,9 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
-    if args.workload == "serve":
-        return {"impl": "reference", "unavailable": "the reference has no serving loop; its CPU decimal path is "
-                                                    "timed by the other workloads"}
+    if args.workload in ("serve", "text"):
+        return {"impl": "reference", "unavailable": "no CPU counterpart timed for this workload; the reference's "
+                                                    "CPU decimal path is timed by the other workloads"}
     if args.workload == "sin":
         per = args.cpu_seconds / max(1, args.steps)
         rates, sample = [], ""
@@ -1139,7 +1192,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    run = {"batch": run_batch, "query": run_query, "sin": run_sin, "serve": run_serve}.get(args.workload, run_ours)
+    run = {"batch": run_batch, "query": run_query, "sin": run_sin, "serve": run_serve, "text": run_text}.get(
+        args.workload, run_ours)
     res = run(args, rank, world)
     if world > 1:
         import torch.distributed as dist

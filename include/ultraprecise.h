@@ -263,6 +263,30 @@ up_status up_query_launch_noalloc(up_module* m, const up_column* in, int32_t n_i
 up_status up_expr_launch_host(up_module* m, const up_column* host_in, int32_t n_in, int64_t rows,
                               void* host_out, uint32_t* err_word, int64_t chunk_rows);
 
+/* ---------------------------------------------------- decimal text in/out */
+/* Parse decimal text into a compact DECIMAL(precision, scale) column, as the
+ * reference's CSV import does (Decimal(precision, scale, mode, str),
+ * decimal.cu:158-165; StringToDecimal :2980-3025; cast :471-533): field r is
+ * text[offsets[r] .. offsets[r+1]) (DEVICE buffers; offsets has rows+1
+ * entries); an optional '-', digits, at most one '.'; extra fraction digits
+ * are cut off (truncation), missing ones padded.  Other characters flag
+ * UP_ROWERR_DOMAIN (the row stores 0); lost magnitude bits flag
+ * UP_ROWERR_OVERFLOW.  precision <= 1000, fields of up to 1500 digits. */
+up_status up_parse_decimal(const char* text, const int64_t* offsets, int64_t rows, int32_t precision, int32_t scale,
+                           void* out, uint32_t* err_word, void* stream);
+
+/* Characters one formatted value of DECIMAL(precision, .) can need. */
+int32_t up_format_width(int32_t precision, int32_t hex);
+
+/* Format a compact column into fixed-width slots of `width` characters (DEVICE
+ * out_text of rows*width bytes; out_len[r] = characters written, -1 when the
+ * slot is too small).  hex != 0: the reference's output image
+ * (Decimal::GetDecimal, decimal.cu:362-398: sign, 8 upper-case hex digits per
+ * limb from the highest nonzero one, "(fff)" scale); hex == 0: the decimal
+ * string ("-123.4500"), which parses back to the same bytes. */
+up_status up_format_decimal(const void* compact, int64_t rows, int32_t precision, int32_t scale, int32_t hex,
+                            char* out_text, int32_t width, int32_t* out_len, void* stream);
+
 /* ------------------------------------------------------------ utilities */
 /* Measured device facts used by the roofline report. */
 typedef struct up_device_info {

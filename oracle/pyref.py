@@ -178,3 +178,58 @@ def eval_nodes(nodes, root: int, col_types, row_values):
         return v
 
     return ev(root), flags["div0"]
+
+
+# ------------------------------------------------------------ decimal text
+UP_ROWERR_OVERFLOW, UP_ROWERR_DOMAIN = 1, 4
+TEXT_MAX_DIGITS = 1500
+
+
+def parse_decimal(text: bytes, nbytes: int, scale: int):
+    """Text -> compact bytes of a column of scale `scale` (nbytes per value)
+    and its row-error bits.  StringToDecimal (decimal.cu:2980-3025): optional
+    '-', the magnitude is every digit, the scale is the digit count after '.';
+    then Decimal::cast (decimal.cu:471-533): pad with zeros or cut digits off
+    (truncation); ToCompactDecimal (decimal.cu:337-341): low bytes, sign bit.
+    Text the reference would misread (another character, a second '.') is a
+    domain error here and stores zeros."""
+    sign, i = 0, 0
+    if text[:1] == b"-":
+        sign, i = 1, 1
+    mag, frac, dot, digits = 0, 0, False, 0
+    for c in text[i:]:
+        if c == ord(".") and not dot:
+            dot = True
+            continue
+        if not (ord("0") <= c <= ord("9")) or digits >= TEXT_MAX_DIGITS:
+            return bytes(nbytes), UP_ROWERR_DOMAIN
+        mag = mag * 10 + (c - ord("0"))
+        digits += 1
+        frac += 1 if dot else 0
+    if scale >= frac:
+        mag *= 10 ** (scale - frac)
+    else:
+        mag //= 10 ** (frac - scale)
+    err = UP_ROWERR_OVERFLOW if mag >> (8 * nbytes - 1) else 0
+    low = mag & ((1 << (8 * nbytes)) - 1)
+    b = bytearray(low.to_bytes(nbytes, "little"))
+    b[-1] |= sign << 7
+    return bytes(b), err
+
+
+def format_decimal(raw: bytes, scale: int, hex_image: bool = False) -> str:
+    """Compact bytes -> text.  hex_image: Decimal::GetDecimal
+    (decimal.cu:362-398), sign, 8 upper-case hex digits per 32-bit limb from
+    the highest nonzero one, "(fff)"; else the decimal string with a '.'
+    before the last `scale` digits and '-' when the sign bit is set."""
+    sign, mag, _ = decode(raw, scale)
+    if hex_image:
+        limbs = []
+        while mag:
+            limbs.append(mag & M32)
+            mag >>= 32
+        body = "".join("%08X" % w for w in reversed(limbs))
+        return ("-" if sign else "+") + body + "(%03d)" % scale
+    digits = str(mag).rjust(scale + 1, "0")
+    body = digits[:-scale] + "." + digits[-scale:] if scale > 0 else digits
+    return ("-" if sign else "") + body

@@ -123,6 +123,9 @@ SIGNATURES = {
     "up_module_result_type": (_I32, [_P, _PI32, _PI32, _PI32]),
     "up_module_source": (_I64, [_P, C.c_char_p, _I64]),
     "up_expr_launch": (_I32, [_P, _P, _I32, _I64, _P, _P, _P]),
+    "up_parse_decimal": (_I32, [_P, _P, _I64, _I32, _I32, _P, _P, _P]),
+    "up_format_width": (_I32, [_I32, _I32]),
+    "up_format_decimal": (_I32, [_P, _I64, _I32, _I32, _I32, _P, _I32, _P, _P]),
     "up_expr_launch_host": (_I32, [_P, _P, _I32, _I64, _P, C.POINTER(C.c_uint32), _I64]),
     "up_module_release": (None, [_P]),
     "up_module_cache_size": (_I32, [_I32]),

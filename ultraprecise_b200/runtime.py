@@ -226,3 +226,48 @@ def group_ids_from_keys(keys: Sequence[torch.Tensor], key_bytes: Sequence[int], 
     abi.check(lib.up_group_ids_from_keys(kp, kb, len(keys), rows, gid.data_ptr(), C.byref(n), gkeys.data_ptr(),
                                          _stream_ptr(stream)), "up_group_ids_from_keys")
     return gid, n.value, gkeys[: n.value * total]
+
+
+def _text_buffers(fields: Sequence[bytes]):
+    import numpy as np
+    lens = np.fromiter((len(f) for f in fields), dtype=np.int64, count=len(fields))
+    offsets = np.zeros(len(fields) + 1, dtype=np.int64)
+    np.cumsum(lens, out=offsets[1:])
+    text = np.frombuffer(b"".join(fields) or b"\0", dtype=np.uint8)
+    return torch.from_numpy(text.copy()).cuda(), torch.from_numpy(offsets).cuda()
+
+
+def parse_decimal(fields: Sequence[bytes], precision: int, scale: int, text: torch.Tensor | None = None,
+                  offsets: torch.Tensor | None = None, stream=None):
+    """Decimal text -> a compact DECIMAL(precision, scale) column on the GPU
+    (up_parse_decimal).  Either byte strings, or device `text` (uint8) and
+    `offsets` (int64, rows+1).  Returns (compact uint8 tensor, row-error word)."""
+    lib = abi.load()
+    if text is None:
+        text, offsets = _text_buffers(fields)
+    rows = offsets.numel() - 1
+    out = torch.empty(max(1, rows * codec.compact_bytes(precision)), dtype=torch.uint8, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    abi.check(lib.up_parse_decimal(text.data_ptr(), offsets.data_ptr(), rows, precision, scale, out.data_ptr(),
+                                   err.data_ptr(), _stream_ptr(stream)), "up_parse_decimal")
+    return out[:rows * codec.compact_bytes(precision)], int(err.item())
+
+
+def format_decimal(col: torch.Tensor, rows: int, precision: int, scale: int, hex_image: bool = False,
+                   stream=None):
+    """A compact column -> (device text slots uint8 [rows, width], lengths int32)
+    (up_format_decimal)."""
+    lib = abi.load()
+    width = lib.up_format_width(precision, 1 if hex_image else 0)
+    text = torch.empty((max(1, rows), width), dtype=torch.uint8, device="cuda")
+    lens = torch.empty(max(1, rows), dtype=torch.int32, device="cuda")
+    abi.check(lib.up_format_decimal(col.data_ptr(), rows, precision, scale, 1 if hex_image else 0, text.data_ptr(),
+                                    width, lens.data_ptr(), _stream_ptr(stream)), "up_format_decimal")
+    return text[:rows], lens[:rows]
+
+
+def format_strings(col: torch.Tensor, rows: int, precision: int, scale: int, hex_image: bool = False) -> list:
+    """format_decimal, copied back as Python strings."""
+    text, lens = format_decimal(col, rows, precision, scale, hex_image)
+    t, ln = text.cpu().numpy(), lens.cpu().numpy()
+    return [bytes(t[i, :ln[i]]).decode() for i in range(rows)]
