@@ -87,6 +87,8 @@ enum {
     UP_NODE_GE = 13,
     UP_NODE_EQ = 14,
     UP_NODE_NE = 15,
+    UP_NODE_AND = 16,     /* AND / OR of two boolean nodes (comparisons or AND/OR): one byte per row, */
+    UP_NODE_OR = 17,      /* the reference's and_or_expr kernels (AriesExprCalcNode.cpp:667-760) */
     UP_NODE_RESCALE = 20  /* extension: truncate toward zero (or widen) to `scale` */
 };
 
@@ -286,6 +288,14 @@ int32_t up_format_width(int32_t precision, int32_t hex);
  * string ("-123.4500"), which parses back to the same bytes. */
 up_status up_format_decimal(const void* compact, int64_t rows, int32_t precision, int32_t scale, int32_t hex,
                             char* out_text, int32_t width, int32_t* out_len, void* stream);
+
+/* --------------------------------------------------------------- filters */
+/* Row selection (FilterFlags / FilterAssociated, AriesSqlOperator_filter.h:15-19):
+ * the indices of the rows whose flag byte is nonzero, in row order, into
+ * `indices` (DEVICE, room for `rows` entries); *count (DEVICE int64) receives
+ * how many.  `flags` is typically the output of a module whose root is a
+ * comparison or an AND/OR of comparisons.  rows <= 2^31-1. */
+up_status up_filter_flags(const uint8_t* flags, int64_t rows, int32_t* indices, int64_t* count, void* stream);
 
 /* ------------------------------------------------------------ utilities */
 /* Measured device facts used by the roofline report. */

@@ -170,6 +170,12 @@ def eval_nodes(nodes, root: int, col_types, row_values):
             v = compare(kind - 10, ev(nd.left), ev(nd.right))
             memo[k] = v
             return v
+        elif kind in (16, 17):
+            # AND / OR of boolean children (AEExprAndOrNode, AriesExprCalcNode.cpp:667-760)
+            lv, rv = ev(nd.left), ev(nd.right)
+            v = int(bool(lv) and bool(rv)) if kind == 16 else int(bool(lv) or bool(rv))
+            memo[k] = v
+            return v
         else:
             raise ValueError(kind)
         if nd.reverse:

@@ -493,7 +493,9 @@ typedef struct {
     uint32_t err;
 } eval_ctx;
 
-static int is_compare(int32_t k) { return k >= UP_NODE_LT && k <= UP_NODE_NE; }
+/* boolean nodes: comparisons, and AND/OR of booleans (AEExprAndOrNode,
+ * AriesExprCalcNode.cpp:667-760; non-null values only) */
+static int is_compare(int32_t k) { return k >= UP_NODE_LT && k <= UP_NODE_OR; }
 
 static int col_value_bytes(const up_col_type* t) {
     return orc_compact_bytes(t->precision) + (t->nullable ? 1 : 0);
@@ -550,7 +552,13 @@ static int eval_node(eval_ctx* c, int32_t idx, int64_t row) {
         default:
             if (is_compare(nd->kind)) {
                 if (eval_node(c, nd->left, row) || eval_node(c, nd->right, row)) return -1;
-                int v = orc_compare(nd->kind, &c->vals[nd->left], &c->vals[nd->right]);
+                int v;
+                if (nd->kind == UP_NODE_AND || nd->kind == UP_NODE_OR) {
+                    const int l = c->vals[nd->left].n != 0, r = c->vals[nd->right].n != 0;
+                    v = nd->kind == UP_NODE_AND ? (l && r) : (l || r);
+                } else {
+                    v = orc_compare(nd->kind, &c->vals[nd->left], &c->vals[nd->right]);
+                }
                 dec_zero(out);
                 out->m[0] = (uint32_t)v;
                 out->n = v ? 1 : 0;

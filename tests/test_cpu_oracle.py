@@ -148,3 +148,26 @@ def test_tables_match_reference_values():
         assert lib.up_precision_words(p) == o.orc_precision_words(p)
         # a compact field always holds every p-digit magnitude
         assert 8 * lib.up_compact_bytes(p) - 1 >= (10 ** p - 1).bit_length()
+
+
+@pytest.mark.parametrize("conn", ["and_", "or_"])
+def test_oracle_and_or(conn):
+    """AND / OR of comparisons, nested, with a division under one side so the
+    division-by-zero flag of either child is kept."""
+    rng = random.Random(11)
+    cols = [E.ColType(18, 4), E.ColType(15, 2), E.ColType(30, 10)]
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    expr = getattr(a.lt(b), conn)(c.ge(a / b).or_(b.eq(0)))
+    n = 150
+    vals = [edge_values(18, rng, n), edge_values(15, rng, n), edge_values(30, rng, n)]
+    run_both(expr, cols, vals, n)
+
+
+def test_boolean_typing_rejects_mixed_children():
+    from ultraprecise_b200 import abi as A
+    a, b = E.col(0), E.col(1)
+    cols = [E.ColType(10, 2), E.ColType(10, 2)]
+    for bad in (a.and_(b), a.lt(b).or_(b), a.lt(b).lt(a.gt(b)), a + a.lt(b)):
+        built = E.build([bad], cols)
+        with pytest.raises(A.UpError):
+            E.derive_types(built)

@@ -28,7 +28,7 @@ GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CXX_SOURCES = ["up_host.cpp", "up_typing.cpp", "up_align.cpp", "up_codegen.cpp", "up_jit.cpp", "up_abi.cpp",
                "up_batch.cpp", "up_serve.cpp"]
-CU_SOURCES = ["up_kernels.cu", "up_noalloc.cu", "up_text.cu"]
+CU_SOURCES = ["up_kernels.cu", "up_noalloc.cu", "up_text.cu", "up_filter.cu"]
 HEADERS = ["up_internal.h", "up_kernels.h", "up_dev.cuh", "up_batch.h"]
 
 

@@ -33,7 +33,7 @@ std::string limbs_init(const Big& x, int n) {
     return s + "}";
 }
 
-bool is_compare_kind(int k) { return k >= UP_NODE_LT && k <= UP_NODE_NE; }
+bool is_compare_kind(int k) { return k >= UP_NODE_LT && k <= UP_NODE_OR; }  // boolean nodes
 
 // Emits the body of a per-row evaluation function for a set of nodes.
 struct Emitter {
@@ -174,6 +174,11 @@ struct Emitter {
                 break;
             }
             default: {
+                if (nd.kind == UP_NODE_AND || nd.kind == UP_NODE_OR) {
+                    body << "    const u32 c" << k << " = c" << nd.left << (nd.kind == UP_NODE_AND ? " & " : " | ") << "c"
+                         << nd.right << ";\n";
+                    return;
+                }
                 // comparison
                 const int sc = std::max(f[nd.left].scale, f[nd.right].scale);
                 std::string A = aligned(nd.left, sc);
@@ -359,6 +364,11 @@ struct TEmitter {
                      << s(nd.left) << ", " << v(nd.right) << ", " << s(nd.right) << ");\n";
                 break;
             default: {
+                if (nd.kind == UP_NODE_AND || nd.kind == UP_NODE_OR) {
+                    body << "    const u32 c" << k << " = c" << nd.left << (nd.kind == UP_NODE_AND ? " & " : " | ") << "c"
+                         << nd.right << ";\n";
+                    return;
+                }
                 const int sc = std::max(f[nd.left].scale, f[nd.right].scale);
                 const std::string A = aligned(nd.left, sc);
                 const std::string Bn = aligned(nd.right, sc);
@@ -421,6 +431,7 @@ int cooperative_width(const up_expr_node* nodes, const std::vector<NodeFacts>& f
                 break;
             default:
                 if (!is_compare_kind(nd.kind)) return 0;
+                if (nd.kind == UP_NODE_AND || nd.kind == UP_NODE_OR) break;
                 {
                     const int sc = std::max(f[nd.left].scale, f[nd.right].scale);
                     for (int o : {nd.left, nd.right}) {

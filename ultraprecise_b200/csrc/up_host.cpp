@@ -231,7 +231,8 @@ void mkdir_if_missing(const std::string& dir) {
 // ------------------------------------------------------ node analysis
 int limbs_for_bits(int bits) { return std::max(1, (bits + 31) / 32); }
 
-static bool is_compare_kind(int k) { return k >= UP_NODE_LT && k <= UP_NODE_NE; }
+// boolean-valued nodes: comparisons and AND/OR
+static bool is_compare_kind(int k) { return k >= UP_NODE_LT && k <= UP_NODE_OR; }
 
 // Static scale of each node as the reference evaluates it: columns carry
 // their scale, constants theirs, integers 0; ADD/SUB take the larger scale
@@ -363,8 +364,11 @@ up_status analyze_nodes(const up_expr_node* nodes, int n_nodes, const up_col_typ
                     if (is_compare_kind(nd.kind)) {
                         const NodeFacts& a = facts[nd.left];
                         const NodeFacts& b = facts[nd.right];
-                        if (a.is_compare || b.is_compare)
+                        const bool logic = nd.kind == UP_NODE_AND || nd.kind == UP_NODE_OR;
+                        if (!logic && (a.is_compare || b.is_compare))
                             return fail(UP_ERR_INVALID_ARG, "comparison of comparisons");
+                        if (logic && !(a.is_compare && b.is_compare))
+                            return fail(UP_ERR_INVALID_ARG, "AND/OR of a non-boolean operand");
                         f.scale = 0;
                         f.bits = 1;
                         f.is_compare = true;

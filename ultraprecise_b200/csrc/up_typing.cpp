@@ -7,7 +7,7 @@
 
 namespace upi {
 
-static bool is_cmp(int k) { return k >= UP_NODE_LT && k <= UP_NODE_NE; }
+static bool is_cmp(int k) { return k >= UP_NODE_LT && k <= UP_NODE_OR; }  // boolean nodes
 
 // ADD/SUB: p = max(p1-s1, p2-s2) + 1 + max(s1, s2), s = max(s1, s2)  (:115-121)
 // MUL:     p = (p1-s1) + (p2-s2) + s1 + s2,        s = s1 + s2       (:122-128)

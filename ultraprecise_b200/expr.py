@@ -82,6 +82,13 @@ class Expr:
     def ne(self, o):
         return self._bin(abi.UP_NODE_NE, o)
 
+    # boolean connectives over comparisons -----------------------------
+    def and_(self, o):
+        return self._bin(abi.UP_NODE_AND, o)
+
+    def or_(self, o):
+        return self._bin(abi.UP_NODE_OR, o)
+
 
 def _wrap(o) -> Expr:
     if isinstance(o, Expr):

@@ -271,3 +271,14 @@ def format_strings(col: torch.Tensor, rows: int, precision: int, scale: int, hex
     text, lens = format_decimal(col, rows, precision, scale, hex_image)
     t, ln = text.cpu().numpy(), lens.cpu().numpy()
     return [bytes(t[i, :ln[i]]).decode() for i in range(rows)]
+
+
+def filter_flags(flags: torch.Tensor, rows: int, stream=None) -> torch.Tensor:
+    """Indices (int32, in row order) of the rows whose flag byte is nonzero
+    (up_filter_flags)."""
+    lib = abi.load()
+    idx = torch.empty(max(1, rows), dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    abi.check(lib.up_filter_flags(flags.data_ptr(), rows, idx.data_ptr(), cnt.data_ptr(), _stream_ptr(stream)),
+              "up_filter_flags")
+    return idx[:int(cnt.item())]
