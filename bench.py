@@ -522,7 +522,7 @@ def cpu_baseline_batch(tasks, cpu_seconds):
 
 # ------------------------------------------------------------ query workload
 QUERY_METRIC = "decimal rows/s (fused grouped SUM/AVG/COUNT query over DECIMAL(15,2)), bit-exact"
-QUERY_BYTES_PER_ROW = 4 * 7 + 4  # four 7-byte decimal columns and the int32 group id
+QUERY_BYTES_PER_ROW = 4 * 7 + 2  # four 7-byte decimal columns and two 1-byte keys
 
 
 def query_inputs(rows, seed, stream=None):
@@ -542,6 +542,10 @@ def query_inputs(rows, seed, stream=None):
 
 
 def run_query(args, rank, world):
+    """One step = the whole grouped query from the raw columns: the key table
+    from the two CHAR(1) key columns (one pass over the key bytes), then the
+    fused query kernel, which reads the key bytes itself and maps them through
+    the table (no group-id array)."""
     import torch
     from ultraprecise_b200 import abi, runtime, workloads
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -551,80 +555,93 @@ def run_query(args, rank, world):
     exprs, aggs, ctypes_ = workloads.query_exprs()
     q = runtime.compile_query(exprs, aggs, ctypes_)
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    table = torch.empty(abi.UP_KEY_TABLE_ENTRIES, dtype=torch.int32, device="cuda")
+    keyb = [1, 1]
     results = {}
+
+    def timed(fn, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
     for label, rows in (("1M", 1 << 20), ("256M", max(1, int((256 << 20) * args.rows_scale)))):
         with torch.cuda.stream(stream):
             cols, k1, k2 = query_inputs(rows, 20261203 + 7 * rank, stream)
             torch.cuda.synchronize()
-            gid, G, _ = runtime.group_ids_from_keys([k1, k2], [1, 1], stream=stream)  # warm (module load)
-            gid_ms = 1e30
-            for _ in range(3):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                gid, G, _ = runtime.group_ids_from_keys([k1, k2], [1, 1], stream=stream)
-                e1.record(stream)
-                torch.cuda.synchronize()
-                gid_ms = min(gid_ms, e0.elapsed_time(e1))
+            _, G, _ = runtime.group_table_from_keys([k1, k2], keyb, stream=stream, table=table)
         dc = [runtime.DeviceColumn(c, 15, 2) for c in cols]
         outs = [torch.empty(G * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES), dtype=torch.uint8,
                             device="cuda") for k, _ in aggs]
 
         def step():
-            q.launch(dc, gid, G, outs=outs, err=err, stream=stream)
+            _, g, _ = runtime.group_table_from_keys([k1, k2], keyb, stream=stream, table=table, distinct=False)
+            q.launch_keys(dc, [k1, k2], keyb, table, g, outs=outs, err=err, stream=stream)
+
+        def kernel_only():
+            q.launch_keys(dc, [k1, k2], keyb, table, G, outs=outs, err=err, stream=stream)
 
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
         barrier(world)
         steps = args.steps
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(dev) as clk:
-            e0.record(stream)
-            for _ in range(steps):
-                step()
-            e1.record(stream)
-            torch.cuda.synchronize()
-        ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
-        gbs = QUERY_BYTES_PER_ROW * rows / (ms * 1e-3) / 1e9
+            ms = max_over_ranks(timed(step, steps), world)
+        # the fused query kernel alone (table fixed): the roofline figure
+        kms = max_over_ranks(timed(kernel_only, steps), world)
+        # the two-pass pipeline for comparison: group-id array, then the query over it
+        with torch.cuda.stream(stream):
+            gid, _, _ = runtime.group_ids_from_keys([k1, k2], keyb, stream=stream)
+        ids_ms = timed(lambda: (runtime.group_ids_from_keys([k1, k2], keyb, stream=stream),
+                                q.launch(dc, gid, G, outs=outs, err=err, stream=stream)), max(1, min(steps, 5)))
+        del gid
+        gbs = QUERY_BYTES_PER_ROW * rows / (kms * 1e-3) / 1e9
         results[label] = {"rows": rows, "groups": G, "ms_per_step": round(ms, 4),
-                          "rows_per_s": round(rows * world / (ms * 1e-3)), "hbm_gbs": round(gbs, 1),
-                          "hbm_frac": round(gbs / hbm_peak, 4), "group_ids_ms": round(gid_ms, 3),
-                          "clocks": clk.summary()}
+                          "rows_per_s": round(rows * world / (ms * 1e-3)), "query_kernel_ms": round(kms, 4),
+                          "hbm_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
+                          "two_pass_group_ids_ms": round(ids_ms, 4), "clocks": clk.summary()}
         if label == "256M":
             main = results[label]
-            inputs = (cols, k1, k2, gid, G, outs)
+            inputs = (cols, k1, k2, table, G, outs)
         else:
-            del cols, k1, k2, gid, dc, outs
+            del cols, k1, k2, dc, outs
     m = main
     res = {"metric": QUERY_METRIC, "value": m["rows_per_s"], "unit": "rows/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
            "config": {"workload": f"grouped SUMx4/AVGx3/COUNT query, DECIMAL(15,2) x4, 2 CHAR(1) keys, "
-                                  f"{m['rows']} rows (256M roofline run; 1M-row case in 'rows_1m')",
+                                  f"{m['rows']} rows, step = key table + fused query "
+                                  f"(256M roofline run; 1M-row case in 'rows_1m')",
                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world} (no collective)"},
            "roofline": {"bound": "hbm", "achieved": m["hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
-                        "frac": m["hbm_frac"], "traffic": None, "kernel": "up_query_acc + up_query_fin",
+                        "frac": m["hbm_frac"], "traffic": None, "kernel": "up_query_tile_r (+ up_query_fin)",
                         "peak_source": peak_kind, "bytes_per_row": QUERY_BYTES_PER_ROW},
-           "rows_1m": results["1M"], "gpu_launches": 2 * args.steps, "clocks": m["clocks"]}
+           "detail": {k: m[k] for k in ("query_kernel_ms", "two_pass_group_ids_ms", "groups")},
+           "rows_1m": results["1M"], "gpu_launches": 4 * args.steps, "clocks": m["clocks"]}
     if not args.no_e2e:
         res["e2e"] = e2e_query(args, q, aggs, inputs, world, stream)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         rate, rows = query_cpu_rate(args.cpu_seconds, os.cpu_count() or 1)
         res["cpu_baseline"] = {"value": round(rate), "unit": "rows/s", "cores": os.cpu_count() or 1,
-                               "kind": "port", "sample": f"{rows} rows of the same query, oracle on "
-                                                         f"{os.cpu_count() or 1} host threads"}
+                               "kind": "port", "sample": f"{rows} rows of the same query (group ids given), "
+                                                         f"oracle on {os.cpu_count() or 1} host threads"}
     return res
 
 
 def e2e_query(args, q, aggs, inputs, world, stream):
     """The query through the C ABI with HOST buffers: per step the four
-    decimal columns and the group ids are copied from pinned host memory, the
-    query runs, and the eight aggregate outputs are copied back."""
+    decimal columns and the two key columns are copied from pinned host
+    memory, the key table is built, the fused query runs, and the eight
+    aggregate outputs are copied back."""
     import torch
     from ultraprecise_b200 import runtime
-    cols, k1, k2, gid, G, outs = inputs
+    cols, k1, k2, table, G, outs = inputs
     pairs = []
-    for d in list(cols) + [gid]:
+    for d in list(cols) + [k1, k2]:
         h = torch.empty(d.numel(), dtype=d.dtype, pin_memory=True)
         h.copy_(d)
         pairs.append((d, h))
@@ -637,7 +654,8 @@ def e2e_query(args, q, aggs, inputs, world, stream):
         with torch.cuda.stream(stream):
             for d, h in pairs:
                 d.copy_(h, non_blocking=True)
-            q.launch(dc, gid, G, outs=outs, stream=stream)
+            _, g, _ = runtime.group_table_from_keys([k1, k2], [1, 1], stream=stream, table=table, distinct=False)
+            q.launch_keys(dc, [k1, k2], [1, 1], table, g, outs=outs, stream=stream)
             for h, o in zip(hout, outs):
                 h.copy_(o, non_blocking=True)
 
@@ -652,7 +670,7 @@ def e2e_query(args, q, aggs, inputs, world, stream):
     t1.record(stream)
     torch.cuda.synchronize()
     ms = max_over_ranks(t0.elapsed_time(t1), world) / steps
-    rows = gid.numel()
+    rows = k1.numel()
     return {"value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": steps}
 

@@ -223,6 +223,28 @@ up_status up_group_ids_from_keys(const void* const* key_cols, const int32_t* key
                                  int32_t n_keys, int64_t rows, int32_t* group_ids,
                                  int32_t* n_groups, void* group_keys, void* stream);
 
+/* The grouping of up_group_ids_from_keys without the per-row id array: one
+ * pass over the key bytes marks the keys present, and `key_table` (DEVICE
+ * int32, UP_KEY_TABLE_ENTRIES entries) receives in entries [0, 65536) each
+ * possible key's dense id in ascending key order (-1 where absent) and in
+ * entries [65536, 65536 + n_groups) the key of each id.  A key is its bytes
+ * in column order, most significant first.  Synchronises `stream` to return
+ * *n_groups. */
+#define UP_KEY_TABLE_ENTRIES 131072
+up_status up_group_table_from_keys(const void* const* key_cols, const int32_t* key_bytes,
+                                   int32_t n_keys, int64_t rows, int32_t* key_table,
+                                   int32_t* n_groups, void* group_keys, void* stream);
+
+/* up_query_launch with the GROUP BY keys read by the query kernel itself
+ * (GroupColumns + AggregateColumnData fused, AriesSqlOperator_group.cu:14-54,
+ * 360-424): each row's group is key_table[key] of its key bytes, so no group
+ * id array is written or read.  Key columns: one of 1 or 2 bytes, or two of 1
+ * byte (DEVICE); key_table and n_groups from up_group_table_from_keys. */
+up_status up_query_launch_keys(up_module* query, const up_column* in, int32_t n_in, int64_t rows,
+                               const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                               const int32_t* key_table, int32_t n_groups, void* const* outs,
+                               uint32_t* err_word, void* stream);
+
 /* ------------------------------------- fused expression + group aggregate */
 typedef struct up_query_agg {
     int32_t kind;       /* UP_AGG_* */

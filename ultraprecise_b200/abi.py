@@ -41,6 +41,7 @@ UP_NODE_NE = 15
 UP_NODE_AND = 16
 UP_NODE_OR = 17
 UP_NODE_RESCALE = 20
+UP_KEY_TABLE_ENTRIES = 131072
 COMPARE_KINDS = (UP_NODE_LT, UP_NODE_LE, UP_NODE_GT, UP_NODE_GE, UP_NODE_EQ, UP_NODE_NE, UP_NODE_AND, UP_NODE_OR)
 
 UP_CONST_MAX_LIMBS = 128
@@ -125,6 +126,8 @@ SIGNATURES = {
     "up_module_result_type": (_I32, [_P, _PI32, _PI32, _PI32]),
     "up_module_source": (_I64, [_P, C.c_char_p, _I64]),
     "up_expr_launch": (_I32, [_P, _P, _I32, _I64, _P, _P, _P]),
+    "up_group_table_from_keys": (_I32, [_P, _P, _I32, _I64, _P, _PI32, _P, _P]),
+    "up_query_launch_keys": (_I32, [_P, _P, _I32, _I64, _P, _P, _I32, _P, _I32, _P, _P, _P]),
     "up_filter_flags": (_I32, [_P, _I64, _P, _P, _P]),
     "up_parse_decimal": (_I32, [_P, _P, _I64, _I32, _I32, _P, _P, _P]),
     "up_format_width": (_I32, [_I32, _I32]),

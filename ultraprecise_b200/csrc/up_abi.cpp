@@ -46,8 +46,12 @@ struct HUpQArgs {
     uint32_t* err;
     int32_t n_groups;
     int32_t vec_ok;
+    const uint8_t* key0;
+    const uint8_t* key1;
+    const int32_t* key_table;
+    int32_t key_mode;
 };
-static_assert(sizeof(HUpQArgs) == 816, "UpQArgs layout");
+static_assert(sizeof(HUpQArgs) == 848, "UpQArgs layout");
 
 up_status cuda_fail(cudaError_t e, const char* what) {
     cudaGetLastError();
@@ -355,11 +359,12 @@ up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64
 }  // extern "C"
 
 up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
-                          int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread) {
+                          int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread,
+                          const QueryKeys* keys) {
     if (!m || !m->is_query) return fail(UP_ERR_INVALID_ARG, "not a query module");
     if (rows < 0 || n_groups < 0) return fail(UP_ERR_INVALID_ARG, "negative size");
     if (n_groups == 0) return UP_OK;
-    if (rows > 0 && !group_ids) return fail(UP_ERR_INVALID_ARG, "group ids are NULL");
+    if (rows > 0 && !keys && !group_ids) return fail(UP_ERR_INVALID_ARG, "group ids are NULL");
     if (!outs) return fail(UP_ERR_INVALID_ARG, "outputs are NULL");
     const GeneratedModule& g = m->jm.gen;
     HUpQArgs a;
@@ -388,15 +393,24 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
     a.err = err_word;
     a.n_groups = n_groups;
     a.vec_ok = vec_ok ? 1 : 0;
+    bool keys_aligned = aligned16(group_ids);
+    if (keys) {
+        a.key0 = keys->key0;
+        a.key1 = keys->key1;
+        a.key_table = keys->table;
+        a.key_mode = keys->mode;
+        keys_aligned = aligned16(keys->key0) && (keys->mode != 2 || aligned16(keys->key1));
+    }
     void* args[1] = {&a};
     if (e == cudaSuccess && rows > 0) {
         if (contig && g.q_staged) {
             // staged tiles; accumulators in registers, shared memory or global
             // memory by group count
-            const char* name = (g.q_gr > 0 && n_groups <= g.q_gr) ? "up_query_tile_r"
-                               : (n_groups <= g.q_gs)             ? "up_query_tile_s"
-                                                                  : "up_query_tile_g";
-            a.vec_ok = (vec_ok && aligned16(group_ids)) ? 1 : 0;
+            const bool reg = g.q_gr > 0 && n_groups <= g.q_gr;
+            const char* name = reg ? (keys ? "up_query_tile_rk" : "up_query_tile_r")
+                               : (n_groups <= g.q_gs) ? "up_query_tile_s"
+                                                      : "up_query_tile_g";
+            a.vec_ok = (vec_ok && keys_aligned) ? 1 : 0;
             void* k = jit_kernel(*m->jm.ks, name);
             st = set_smem(k, g.q_smem);  // the tile layout is kept within 48 KB: normally a no-op
             if (st != UP_OK) return st;
@@ -502,6 +516,41 @@ up_status up_group_ids_from_keys(const void* const* key_cols, const int32_t* key
     cudaStream_t s = (cudaStream_t)stream;
     UP_CUDA(launch_group_ids_small_keys(key_cols, key_bytes, n_keys, rows, group_ids, n_groups, group_keys, s));
     return UP_OK;
+}
+
+up_status up_group_table_from_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                   int64_t rows, int32_t* key_table, int32_t* n_groups, void* group_keys,
+                                   void* stream) {
+    if (!key_cols || !key_bytes || !key_table || !n_groups) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    if (rows < 0) return fail(UP_ERR_INVALID_ARG, "negative row count");
+    if (n_keys < 1 || n_keys > 4) return fail(UP_ERR_INVALID_ARG, "1..4 key columns");
+    int total = 0;
+    for (int k = 0; k < n_keys; k++) {
+        if (key_bytes[k] < 1) return fail(UP_ERR_INVALID_ARG, "key width < 1");
+        if (rows > 0 && !key_cols[k]) return fail(UP_ERR_INVALID_ARG, "key column is NULL");
+        total += key_bytes[k];
+    }
+    if (total > 2) return fail(UP_ERR_UNSUPPORTED, "direct key table supports at most 2 key bytes in total");
+    UP_CUDA(launch_group_table_small_keys(key_cols, key_bytes, n_keys, rows, key_table, n_groups, group_keys,
+                                          (cudaStream_t)stream));
+    return UP_OK;
+}
+
+up_status up_query_launch_keys(up_module* m, const up_column* in, int32_t n_in, int64_t rows,
+                               const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                               const int32_t* key_table, int32_t n_groups, void* const* outs, uint32_t* err_word,
+                               void* stream) {
+    if (!key_cols || !key_bytes || !key_table) return fail(UP_ERR_INVALID_ARG, "NULL key arguments");
+    QueryKeys k;
+    if (n_keys == 1 && key_bytes[0] == 1) k.mode = 1;
+    else if (n_keys == 2 && key_bytes[0] == 1 && key_bytes[1] == 1) k.mode = 2;
+    else if (n_keys == 1 && key_bytes[0] == 2) k.mode = 3;
+    else return fail(UP_ERR_UNSUPPORTED, "key columns: one of 1 or 2 bytes, or two of 1 byte");
+    k.key0 = (const uint8_t*)key_cols[0];
+    k.key1 = k.mode == 2 ? (const uint8_t*)key_cols[1] : nullptr;
+    k.table = key_table;
+    if (rows > 0 && (!k.key0 || (k.mode == 2 && !k.key1))) return fail(UP_ERR_INVALID_ARG, "key column is NULL");
+    return query_launch_ex(m, in, n_in, rows, nullptr, n_groups, outs, err_word, stream, false, &k);
 }
 
 up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,

@@ -227,6 +227,59 @@ struct UpQArgs {
 )";
 }
 
+// Query modules: UpQArgs with the group-key fields and the group lookup.
+std::string query_kargs_source() {
+    return R"(
+#define UP_MAX_COLS 16
+#define UP_MAX_AGGS 16
+struct UpArgs {
+    KCol col[UP_MAX_COLS];
+    i64 rows;
+    u8* out;
+    u32* err;
+    int vec_ok;
+    int out_nullable;
+};
+struct UpQArgs {
+    KCol col[UP_MAX_COLS];
+    u8* out[UP_MAX_AGGS];
+    i64 rows;
+    const int* gid;
+    u32* acc;
+    u64* cnt;
+    u32* err;
+    int n_groups;
+    int vec_ok;
+    // key_mode 0: group ids from gid[]; otherwise the group is
+    // key_table[key] with key = key0[r] (1), key0[r] << 8 | key1[r] (2), or
+    // key0[2r] << 8 | key0[2r+1] (3)
+    const u8* key0;
+    const u8* key1;
+    const int* key_table;
+    int key_mode;
+};
+UP_DI int q_group(const UpQArgs& a, i64 row) {
+    if (a.key_mode == 0) return a.gid[row];
+    u32 key;
+    if (a.key_mode == 1) key = a.key0[row];
+    else if (a.key_mode == 2) key = ((u32)a.key0[row] << 8) | a.key1[row];
+    else key = ((u32)a.key0[2 * row] << 8) | a.key0[2 * row + 1];
+    return __ldg(a.key_table + key);
+}
+// the key of row r of a staged tile of R rows (key bytes at t)
+UP_DI u32 q_tile_key(const UpQArgs& a, const u8* t, int r, int R) {
+    if (a.key_mode == 1) return t[r];
+    if (a.key_mode == 2) return ((u32)t[r] << 8) | t[R + r];
+    return ((u32)t[2 * r] << 8) | t[2 * r + 1];
+}
+// the group of row r of a staged tile (gid or key bytes at t)
+UP_DI int q_tile_group(const UpQArgs& a, const u8* t, int r, int R) {
+    if (a.key_mode == 0) return ((const int*)t)[r];
+    return __ldg(a.key_table + q_tile_key(a, t, r, R));
+}
+)";
+}
+
 std::string params_decl(const std::vector<int>& used_cols) {
     std::string p;
     for (int c : used_cols) p += "const u8* __restrict__ in" + std::to_string(c) + ", ";
@@ -835,7 +888,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
 
     const int T = (opts && opts->block_threads > 0) ? opts->block_threads : 256;
     std::ostringstream src;
-    src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << kargs_source();
+    src << "#include \"up_dev.cuh\"\nusing namespace up;\n" << query_kargs_source();
     // per row: every accumulated expression as a two's complement image
     src << "UP_DI u32 up_qvals(" << params_decl(used) << "const bool words";
     for (int i = 0; i < NR; i++) src << ", u32 (&qv" << i << ")[" << acc_limbs[i] << "]";
@@ -860,7 +913,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     src << "    u32 err = 0u;\n";
     src << "    const i64 stride = (i64)gridDim.x * blockDim.x;\n";
     src << "    for (i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x; row < a.rows; row += stride) {\n";
-    src << "        const int g = a.gid[row];\n";
+    src << "        const int g = q_group(a, row);\n";
     src << "        if ((unsigned)g >= (unsigned)a.n_groups) { err |= ERR_DOMAIN; continue; }\n";
     src << "        atomicAdd(a.cnt + g, 1ull);\n";
     src << "        bool isnull = false;\n";
@@ -925,7 +978,11 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         out.q_smem = smem;
         int tile_in_bytes = R * 4;
         for (int c : used) tile_in_bytes += R * compact_bytes(cols[c].precision);
-        src << "template <int MODE>\nUP_DI void up_query_tile_body(const UpQArgs& a, u8* sm) {\n";
+        // KEYS (register mode with key columns): a row's key is matched
+        // against the present keys held in registers (the inverse half of the
+        // key table), so no table lookup happens per row; rows matching none
+        // are counted and flagged as a domain error at the end
+        src << "template <int MODE, int KEYS>\nUP_DI void up_query_tile_body(const UpQArgs& a, u8* sm) {\n";
         src << "    constexpr int R = " << R << ";\n    constexpr int W = " << W << ";\n";
         src << "    constexpr int GR = " << std::max(GR, 1) << ";\n";
         src << "    u64* bar = (u64*)(sm + " << off_bar << ");\n";
@@ -946,21 +1003,31 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         for (int i = 0; i < NR; i++)
             src << "#pragma unroll\n        for (int l = 0; l < " << ra_limbs(i) << "; l++) ra" << i << "[j][l] = 0u;\n";
         src << "    }\n";
+        src << "    u32 kj[KEYS ? GR : 1];\n    u32 nrow = 0u;\n";
+        src << "#pragma unroll\n    for (int j = 0; j < (KEYS ? GR : 1); j++)\n";
+        src << "        kj[j] = (KEYS && j < nsm) ? (u32)__ldg(a.key_table + 65536 + j) : 0xffffffffu;\n";
         src << "    const i64 ntiles = (a.rows + R - 1) / R;\n";
         src << "    const i64 nfull = a.vec_ok ? a.rows / R : 0;  // tiles moved by bulk copies\n";
         src << "    u32 err = 0u;\n";
         src << "    if (threadIdx.x == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); mbar_init_fence(); }\n";
         src << "    __syncthreads();\n";
         src << "    auto issue = [&](i64 tt, int st) {\n";
-        src << "        mbar_expect_tx(&bar[st], " << tile_in_bytes << "u);\n";
+        src << "        mbar_expect_tx(&bar[st], " << tile_in_bytes - R * 4
+            << "u + (a.key_mode == 0 ? " << R * 4 << "u : a.key_mode == 1 ? " << R << "u : " << 2 * R << "u));\n";
         for (size_t i = 0; i < used.size(); i++) {
             int c = used[i];
             int B = compact_bytes(cols[c].precision);
             src << "        bulk_load(sm + st * " << stage_in << " + " << off[i] << ", a.col[" << c
                 << "].data + tt * (i64)(R * " << B << "), " << R * B << "u, &bar[st]);\n";
         }
-        src << "        bulk_load(sm + st * " << stage_in << " + " << off_gid
+        src << "        if (a.key_mode == 0) bulk_load(sm + st * " << stage_in << " + " << off_gid
             << ", (const u8*)(a.gid + tt * (i64)R), " << R * 4 << "u, &bar[st]);\n";
+        src << "        else if (a.key_mode == 3) bulk_load(sm + st * " << stage_in << " + " << off_gid
+            << ", a.key0 + tt * (i64)" << 2 * R << ", " << 2 * R << "u, &bar[st]);\n";
+        src << "        else {\n            bulk_load(sm + st * " << stage_in << " + " << off_gid << ", a.key0 + tt * (i64)R, "
+            << R << "u, &bar[st]);\n";
+        src << "            if (a.key_mode == 2) bulk_load(sm + st * " << stage_in << " + " << off_gid + R
+            << ", a.key1 + tt * (i64)R, " << R << "u, &bar[st]);\n        }\n";
         src << "    };\n";
         src << "    if (threadIdx.x == 0 && (i64)blockIdx.x < nfull) issue(blockIdx.x, 0);\n";
         src << "    int k = 0;\n";
@@ -982,14 +1049,22 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
             src << "            tile_copy_in(in + " << off[i] << ", a.col[" << c << "].data + row0 * " << B << ", nr * "
                 << B << ", a.vec_ok != 0);\n";
         }
-        src << "            tile_copy_in(in + " << off_gid << ", (const u8*)(a.gid + row0), nr * 4, a.vec_ok != 0);\n";
+        src << "            if (a.key_mode == 0) tile_copy_in(in + " << off_gid
+            << ", (const u8*)(a.gid + row0), nr * 4, a.vec_ok != 0);\n";
+        src << "            else if (a.key_mode == 3) tile_copy_in(in + " << off_gid
+            << ", a.key0 + row0 * 2, nr * 2, a.vec_ok != 0);\n";
+        src << "            else {\n                tile_copy_in(in + " << off_gid << ", a.key0 + row0, nr, a.vec_ok != 0);\n";
+        src << "                if (a.key_mode == 2) tile_copy_in(in + " << off_gid + R
+            << ", a.key1 + row0, nr, a.vec_ok != 0);\n            }\n";
         src << "            __syncthreads();\n";
         src << "        }\n";
         src << "        if (__syncthreads_or(timed_out)) break;\n";
-        src << "        const int* tg = (const int*)(in + " << off_gid << ");\n";
+        src << "        const u8* tg = in + " << off_gid << ";\n";
         src << "        for (int r = threadIdx.x; r < nr; r += blockDim.x) {\n";
-        src << "            const int g = tg[r];\n";
-        src << "            if ((unsigned)g >= (unsigned)ng) { err |= ERR_DOMAIN; continue; }\n";
+        src << "            const u32 key = KEYS ? q_tile_key(a, tg, r, R) : 0u;\n";
+        src << "            const int g = KEYS ? 0 : q_tile_group(a, tg, r, R);\n";
+        src << "            if (!KEYS && (unsigned)g >= (unsigned)ng) { err |= ERR_DOMAIN; continue; }\n";
+        src << "            if (KEYS) nrow++;\n";
         src << decl_t("            ");
         if (NR > 0) {
             src << "            err |= up_qvals(";
@@ -1001,11 +1076,13 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         for (int i = 0; i < NR; i++)
             if (acc_limbs[i] > 4) {
                 src << "                const bool f" << i << " = fits_twos64(qv" << i << ");\n";
-                src << "                if (!f" << i << ") atomic_add_twos(sacc + g * W + " << acc_off[i] << ", qv" << i
-                    << ");  // rare: wider than 64 bits\n";
+                src << "                if (!f" << i << ") {  // rare: wider than 64 bits\n";
+                src << "                    const int gw = KEYS ? __ldg(a.key_table + key) : g;\n";
+                src << "                    if ((unsigned)gw < (unsigned)nsm) atomic_add_twos(sacc + gw * W + " << acc_off[i]
+                    << ", qv" << i << ");\n                }\n";
             }
         src << "#pragma unroll\n                for (int j = 0; j < GR; j++)\n";
-        src << "                    if (g == j) {\n                        rc[j]++;\n";
+        src << "                    if (KEYS ? key == kj[j] : g == j) {\n                        rc[j]++;\n";
         for (int i = 0; i < NR; i++) {
             if (acc_limbs[i] > 4)
                 src << "                        if (f" << i << ") add_twos64(ra" << i << "[j], qv" << i << ");\n";
@@ -1029,6 +1106,9 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         src << "        err |= ERR_TIMEOUT;\n";
         src << "        mbar_wait(&bar[to_st], to_par);  // bounded: let copies in flight land before exit\n";
         src << "    }\n";
+        src << "    if constexpr (MODE == 0 && KEYS) {\n        u32 matched = 0u;\n";
+        src << "#pragma unroll\n        for (int j = 0; j < GR; j++) matched += rc[j];\n";
+        src << "        if (matched != nrow) err |= ERR_DOMAIN;  // a key outside the table\n    }\n";
         src << "    if constexpr (MODE == 0) {\n";
         src << "#pragma unroll\n        for (int j = 0; j < GR; j++)\n";
         src << "            if (rc[j] != 0u) {\n";
@@ -1062,12 +1142,16 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
         src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n";
         src << "}\n\n";
-        const char* names[3] = {"up_query_tile_r", "up_query_tile_s", "up_query_tile_g"};
-        for (int mde = 0; mde < 3; mde++) {
+        const char* names[4] = {"up_query_tile_r", "up_query_tile_s", "up_query_tile_g", "up_query_tile_rk"};
+        for (int kn = 0; kn < 4; kn++) {
+            const int mde = kn == 3 ? 0 : kn;
             if (mde == 0 && GR == 0) continue;
-            src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") " << names[mde]
+            // two CTAs per SM for the register modes (the key-matching one
+            // would otherwise take a few registers too many for that)
+            src << "extern \"C\" __global__ void __launch_bounds__(" << T << (mde == 0 && T == 256 ? ", 2" : "") << ") "
+                << names[kn]
                 << "(const UpQArgs a) {\n    extern __shared__ __align__(128) u8 sm[];\n    up_query_tile_body<" << mde
-                << ">(a, sm);\n}\n\n";
+                << ", " << (kn == 3 ? 1 : 0) << ">(a, sm);\n}\n\n";
         }
     }
 
@@ -1110,7 +1194,10 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     out.work_per_row = em.work + row_bytes;
     out.kernels = {"up_query_acc", "up_query_fin"};
     if (out.q_staged) {
-        if (out.q_gr > 0) out.kernels.push_back("up_query_tile_r");
+        if (out.q_gr > 0) {
+            out.kernels.push_back("up_query_tile_r");
+            out.kernels.push_back("up_query_tile_rk");
+        }
         out.kernels.push_back("up_query_tile_s");
         out.kernels.push_back("up_query_tile_g");
     }

@@ -189,7 +189,16 @@ struct up_module {
 // often and higher-priority streams get SMs between them.
 up_status expr_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, void* out,
                          uint32_t* err_word, void* stream, bool spread);
+// Group keys read by the query kernel itself (key_mode 1..3 of the generated
+// UpQArgs) instead of a group id array.
+struct QueryKeys {
+    const uint8_t* key0 = nullptr;
+    const uint8_t* key1 = nullptr;
+    const int32_t* table = nullptr;
+    int mode = 0;
+};
 up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
-                          int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread);
+                          int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread,
+                          const QueryKeys* keys = nullptr);
 
 #endif  // UP_INTERNAL_H_

@@ -75,10 +75,16 @@ cudaError_t launch_division_int64(const uint8_t* sums, const int64_t* counts, in
 }
 
 // --------------------------------------------------- small-key grouping
+// Keys of at most 2 bytes in total.  A row's key is its key bytes in column
+// order, most significant first, so ascending keys are the order of the
+// reference's sort-based GroupColumns (AriesSqlOperator_group.cu:14-54).
+// The key table maps each of the 65536 possible keys to its dense group id
+// (-1 for an absent key); its second half lists the present keys by id.
 struct KeyCols {
     const u8* col[4];
     int bytes[4];
     int n;
+    int fast16;  // 1 or 2 one-byte key columns, 16-byte aligned
 };
 
 __device__ __forceinline__ u32 row_key(const KeyCols& k, int64_t row) {
@@ -88,82 +94,174 @@ __device__ __forceinline__ u32 row_key(const KeyCols& k, int64_t row) {
     return key;
 }
 
-__global__ void k_mark_keys(KeyCols k, int64_t rows, u32* __restrict__ flags) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) {
-        const u32 key = row_key(k, i);
-        if (flags[key] == 0u) flags[key] = 1u;
-    }
+constexpr int kKeyWords = 65536 / 32;  // words of the key presence bitmap
+
+__device__ __forceinline__ void mark_key(u32* sb, u32 key) {
+    const u32 m = 1u << (key & 31u);
+    if (!(sb[key >> 5] & m)) atomicOr(&sb[key >> 5], m);
 }
 
-// one block: exclusive scan of 65536 presence flags -> dense ids in key order
-__global__ void __launch_bounds__(1024) k_scan_keys(const u32* __restrict__ flags, int32_t* __restrict__ ids,
+// Every block marks the keys of its rows in a shared-memory bitmap (one-byte
+// key columns are read 16 rows per 16-byte load), then ORs its nonzero words
+// into the global bitmap.
+__global__ void __launch_bounds__(256) k_mark_keys(KeyCols k, int64_t rows, u32* __restrict__ bits) {
+    __shared__ u32 sb[kKeyWords];
+    for (int i = threadIdx.x; i < kKeyWords; i += blockDim.x) sb[i] = 0u;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t done = 0;
+    if (k.fast16) {
+        const int64_t nvec = rows / 16;
+        const uint4* a = (const uint4*)k.col[0];
+        const uint4* b = (const uint4*)k.col[1];
+        // two vectors per column in flight per thread, then 32 marks
+        for (int64_t v = tid; v < nvec; v += 2 * stride) {
+            const bool two = v + stride < nvec;
+            uint4 x[2], y[2];
+            x[0] = a[v];
+            x[1] = two ? a[v + stride] : x[0];
+            y[0] = k.n == 2 ? b[v] : make_uint4(0u, 0u, 0u, 0u);
+            y[1] = k.n == 2 && two ? b[v + stride] : y[0];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const u32 xw[4] = {x[h].x, x[h].y, x[h].z, x[h].w}, yw[4] = {y[h].x, y[h].y, y[h].z, y[h].w};
+#pragma unroll
+                for (int w = 0; w < 4; w++) {
+                    if (k.n == 2) {
+                        // two 16-bit keys per word: bytes (lo, hi) of rows 0-1, then rows 2-3
+                        const u32 p01 = __byte_perm(xw[w], yw[w], 0x1504u);
+                        const u32 p23 = __byte_perm(xw[w], yw[w], 0x3726u);
+                        mark_key(sb, p01 & 0xffffu);
+                        mark_key(sb, p01 >> 16);
+                        mark_key(sb, p23 & 0xffffu);
+                        mark_key(sb, p23 >> 16);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 4; j++) mark_key(sb, (xw[w] >> (8 * j)) & 0xffu);
+                    }
+                }
+            }
+        }
+        done = nvec * 16;
+    }
+    for (int64_t i = done + tid; i < rows; i += stride) mark_key(sb, row_key(k, i));
+    __syncthreads();
+    for (int i = threadIdx.x; i < kKeyWords; i += blockDim.x)
+        if (sb[i]) atomicOr(&bits[i], sb[i]);
+}
+
+// one block: dense ids in key order from the presence bitmap (64 keys per
+// thread), the key table, the group count and the distinct keys
+__global__ void __launch_bounds__(1024) k_scan_keys(const u32* __restrict__ bits, int32_t* __restrict__ table,
                                                     int32_t* __restrict__ n_out, u8* __restrict__ keys_out,
                                                     int key_bytes) {
     __shared__ int part[1024];
     const int t = threadIdx.x;
-    const int per = 65536 / 1024;
-    int c = 0;
-    for (int j = 0; j < per; j++) c += flags[t * per + j] ? 1 : 0;
+    const u32 w0 = bits[2 * t], w1 = bits[2 * t + 1];
+    const int c = __popc(w0) + __popc(w1);
     part[t] = c;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
-        int v = t >= off ? part[t - off] : 0;
+        const int v = t >= off ? part[t - off] : 0;
         __syncthreads();
         part[t] += v;
         __syncthreads();
     }
     int base = part[t] - c;
-    for (int j = 0; j < per; j++) {
-        const int key = t * per + j;
-        if (flags[key]) {
-            ids[key] = base;
-            if (keys_out) {
-                for (int b = 0; b < key_bytes; b++) keys_out[(int64_t)base * key_bytes + b] =
-                    (u8)(key >> (8 * (key_bytes - 1 - b)));
-            }
+    for (int j = 0; j < 64; j++) {
+        const int key = t * 64 + j;
+        const bool present = (((j < 32 ? w0 : w1) >> (j & 31)) & 1u) != 0u;
+        if (present) {
+            table[key] = base;
+            table[65536 + base] = key;
+            if (keys_out)
+                for (int b = 0; b < key_bytes; b++)
+                    keys_out[(int64_t)base * key_bytes + b] = (u8)(key >> (8 * (key_bytes - 1 - b)));
             base++;
         } else {
-            ids[key] = -1;
+            table[key] = -1;
         }
     }
     if (t == 1023) *n_out = part[1023];
 }
 
-__global__ void k_map_keys(KeyCols k, int64_t rows, const int32_t* __restrict__ ids, int32_t* __restrict__ gid) {
+__global__ void k_map_keys(KeyCols k, int64_t rows, const int32_t* __restrict__ table, int32_t* __restrict__ gid) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride) gid[i] = ids[row_key(k, i)];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += stride)
+        gid[i] = __ldg(table + row_key(k, i));
+}
+
+namespace {
+
+KeyCols key_cols_of(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys, int* total) {
+    KeyCols k;
+    *total = 0;
+    bool fast = n_keys <= 2;
+    for (int c = 0; c < 4; c++) {
+        k.col[c] = c < n_keys ? (const u8*)key_cols[c] : nullptr;
+        k.bytes[c] = c < n_keys ? key_bytes[c] : 0;
+        *total += k.bytes[c];
+        if (c < n_keys) fast = fast && key_bytes[c] == 1 && ((uintptr_t)key_cols[c] & 15u) == 0u;
+    }
+    k.n = n_keys;
+    k.fast16 = fast ? 1 : 0;
+    return k;
+}
+
+// mark + scan into `table`; the group count lands in *dn (device)
+cudaError_t group_table_async(const KeyCols& k, int total, int64_t rows, int32_t* table, int32_t* dn, u32* bits,
+                              void* group_keys, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(bits, 0, kKeyWords * 4, s);
+    if (e != cudaSuccess) return e;
+    if (rows > 0) {
+        const int sms = std::max(1, sm_count_current());
+        const int64_t work = k.fast16 ? (rows + 15) / 16 : rows;
+        const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)sms * 8));
+        k_mark_keys<<<(unsigned)blocks, 256, 0, s>>>(k, rows, bits);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    k_scan_keys<<<1, 1024, 0, s>>>(bits, table, dn, (u8*)group_keys, total);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_group_table_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                          int64_t rows, int32_t* table, int32_t* n_groups, void* group_keys,
+                                          cudaStream_t s) {
+    int total = 0;
+    const KeyCols k = key_cols_of(key_cols, key_bytes, n_keys, &total);
+    void* scratch = nullptr;
+    cudaError_t e = cudaMallocAsync(&scratch, kKeyWords * 4 + 16, s);
+    if (e != cudaSuccess) return e;
+    u32* bits = (u32*)scratch;
+    int32_t* dn = (int32_t*)((u8*)scratch + kKeyWords * 4);
+    e = group_table_async(k, total, rows, table, dn, bits, group_keys, s);
+    int32_t hn = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hn, dn, 4, cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) *n_groups = hn;
+    return e;
 }
 
 cudaError_t launch_group_ids_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
                                         int64_t rows, int32_t* gid, int32_t* n_groups, void* group_keys,
                                         cudaStream_t s) {
-    KeyCols k;
     int total = 0;
-    for (int c = 0; c < 4; c++) {
-        k.col[c] = c < n_keys ? (const u8*)key_cols[c] : nullptr;
-        k.bytes[c] = c < n_keys ? key_bytes[c] : 0;
-        total += k.bytes[c];
-    }
-    k.n = n_keys;
+    const KeyCols k = key_cols_of(key_cols, key_bytes, n_keys, &total);
     void* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, 65536 * 8 + 16, s);
+    cudaError_t e = cudaMallocAsync(&scratch, 65536 * 4 + kKeyWords * 4 + 16, s);
     if (e != cudaSuccess) return e;
-    u32* flags = (u32*)scratch;
-    int32_t* ids = (int32_t*)((u8*)scratch + 65536 * 4);
-    int32_t* dn = (int32_t*)((u8*)scratch + 65536 * 8);
-    e = cudaMemsetAsync(flags, 0, 65536 * 4, s);
-    int64_t blocks = std::min<int64_t>((rows + 255) / 256, 148 * 8);
+    int32_t* table = (int32_t*)scratch;
+    u32* bits = (u32*)((u8*)scratch + 65536 * 4);
+    int32_t* dn = (int32_t*)((u8*)scratch + 65536 * 4 + kKeyWords * 4);
+    e = group_table_async(k, total, rows, table, dn, bits, group_keys, s);
     if (e == cudaSuccess && rows > 0) {
-        k_mark_keys<<<(unsigned)blocks, 256, 0, s>>>(k, rows, flags);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) {
-        k_scan_keys<<<1, 1024, 0, s>>>(flags, ids, dn, (u8*)group_keys, total);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess && rows > 0) {
-        k_map_keys<<<(unsigned)blocks, 256, 0, s>>>(k, rows, ids, gid);
+        const int sms = std::max(1, sm_count_current());
+        const int64_t blocks = std::min<int64_t>((rows + 255) / 256, (int64_t)sms * 8);
+        k_map_keys<<<(unsigned)blocks, 256, 0, s>>>(k, rows, table, gid);
         e = cudaGetLastError();
     }
     int32_t hn = 0;

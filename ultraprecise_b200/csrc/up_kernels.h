@@ -15,6 +15,10 @@ cudaError_t launch_division_int64(const uint8_t* sums, const int64_t* counts, in
 cudaError_t launch_group_ids_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
                                         int64_t rows, int32_t* gid, int32_t* n_groups, void* group_keys,
                                         cudaStream_t s);
+// The 65536-entry key table only (no per-row ids); also synchronises.
+cudaError_t launch_group_table_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                          int64_t rows, int32_t* table, int32_t* n_groups, void* group_keys,
+                                          cudaStream_t s);
 
 }  // namespace upi
 

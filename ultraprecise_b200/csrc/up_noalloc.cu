@@ -92,8 +92,12 @@ struct NaQArgs {
     uint32_t* err;
     int32_t n_groups;
     int32_t vec_ok;
+    const uint8_t* key0;  // key modes are not used here (group ids only)
+    const uint8_t* key1;
+    const int32_t* key_table;
+    int32_t key_mode;
 };
-static_assert(sizeof(NaQArgs) == 816, "UpQArgs layout");
+static_assert(sizeof(NaQArgs) == 848, "UpQArgs layout");
 
 up_status na_cuda(cudaError_t e, const char* what) {
     cudaGetLastError();

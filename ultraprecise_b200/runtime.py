@@ -169,6 +169,26 @@ class QueryModule:
                   "up_query_launch")
         return list(outs)
 
+    def launch_keys(self, cols: Sequence[DeviceColumn], keys: Sequence[torch.Tensor], key_bytes: Sequence[int],
+                    key_table: torch.Tensor, n_groups: int, outs: Sequence[torch.Tensor] | None = None,
+                    err: torch.Tensor | None = None, stream=None, rows: int | None = None) -> list[torch.Tensor]:
+        """The query with its GROUP BY key columns read by the kernel
+        (up_query_launch_keys); key_table / n_groups from group_table_from_keys."""
+        lib = abi.load()
+        if rows is None:
+            rows = keys[0].numel() // key_bytes[0]
+        if outs is None:
+            outs = [torch.empty(n_groups * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES),
+                                dtype=torch.uint8, device="cuda") for k, _ in self.aggs]
+        optr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+        arr = _columns_array(cols)
+        kp = (C.c_void_p * len(keys))(*[k.data_ptr() for k in keys])
+        kb = (C.c_int32 * len(keys))(*key_bytes)
+        abi.check(lib.up_query_launch_keys(self._h, arr, len(cols), rows, kp, kb, len(keys), key_table.data_ptr(),
+                                           n_groups, optr, err.data_ptr() if err is not None else None,
+                                           _stream_ptr(stream)), "up_query_launch_keys")
+        return list(outs)
+
     def __del__(self):
         try:
             abi.load().up_module_release(self._h)
@@ -226,6 +246,25 @@ def group_ids_from_keys(keys: Sequence[torch.Tensor], key_bytes: Sequence[int], 
     abi.check(lib.up_group_ids_from_keys(kp, kb, len(keys), rows, gid.data_ptr(), C.byref(n), gkeys.data_ptr(),
                                          _stream_ptr(stream)), "up_group_ids_from_keys")
     return gid, n.value, gkeys[: n.value * total]
+
+
+def group_table_from_keys(keys: Sequence[torch.Tensor], key_bytes: Sequence[int], stream=None,
+                          table: torch.Tensor | None = None, distinct: bool = True):
+    """The key -> dense group id table (up_group_table_from_keys); returns
+    (table, n_groups, distinct keys or None)."""
+    lib = abi.load()
+    rows = keys[0].numel() // key_bytes[0]
+    if table is None:
+        table = torch.empty(abi.UP_KEY_TABLE_ENTRIES, dtype=torch.int32, device="cuda")
+    total = sum(key_bytes)
+    gkeys = torch.empty(65536 * total, dtype=torch.uint8, device="cuda") if distinct else None
+    kp = (C.c_void_p * len(keys))(*[k.data_ptr() for k in keys])
+    kb = (C.c_int32 * len(keys))(*key_bytes)
+    n = C.c_int32()
+    abi.check(lib.up_group_table_from_keys(kp, kb, len(keys), rows, table.data_ptr(), C.byref(n),
+                                           gkeys.data_ptr() if distinct else None, _stream_ptr(stream)),
+              "up_group_table_from_keys")
+    return table, n.value, (gkeys[: n.value * total] if distinct else None)
 
 
 def _text_buffers(fields: Sequence[bytes]):
