@@ -161,6 +161,13 @@ up_status nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::s
     // shared memory per kernel) and prints the compile log to stderr.
     const char* vb = getenv("UP_JIT_VERBOSE");
     const bool verbose = vb && *vb && *vb != '0';
+    // UP_JIT_DUMP_SOURCE=<file> appends every generated kernel source compiled
+    if (const char* dump = getenv("UP_JIT_DUMP_SOURCE")) {
+        if (FILE* f = fopen(dump, "a")) {
+            fprintf(f, "// ---- generated module ----\n%s\n", src.c_str());
+            fclose(f);
+        }
+    }
     std::vector<const char*> opts = {kArch, "-std=c++17", "-lineinfo", "--restrict", "-DUP_NVRTC=1"};
     if (rdc) opts.push_back("-rdc=true");
     if (verbose) opts.push_back("--ptxas-options=-v");
