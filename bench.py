@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query", "sin", "serve", "text"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query", "sin", "serve", "text", "filter"])
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per rate (serve workload)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1057,6 +1057,135 @@ def run_text(args, rank, world):
             "gpu_launches": 2 * args.steps, "clocks": clk.summary()}
 
 
+# ------------------------------------------------------------ filter workload
+FILTER_METRIC = "decimal rows/s filtered (WHERE a*b >= c AND a <> 0 over DECIMAL(38,9), kept row indices), bit-exact"
+
+
+def filter_cpu_rate(cpu_seconds, threads, seed=9):
+    """Oracle rows/s for the predicate plus numpy's nonzero on the host."""
+    import numpy as np
+    from oracle import gen, oracle
+    from ultraprecise_b200 import expr as E
+    e, ct = filter_expr()
+    b = E.build([e], ct)
+    E.derive_types(b)
+
+    def run(rows):
+        cols = [gen.compact_digits(rows, 38, 16, seed + k) for k in range(3)]
+        t = time.perf_counter()
+        flags, _ = oracle.eval_expr(b, b.roots[0], cols, rows, 1, threads=threads)
+        np.nonzero(np.frombuffer(flags, dtype=np.uint8))
+        return time.perf_counter() - t
+
+    r0 = 1 << 14
+    s0 = run(r0)
+    rows = int(min(1 << 26, r0 * cpu_seconds / max(s0, 1e-4)))
+    return rows / run(rows), rows
+
+
+def filter_expr():
+    from ultraprecise_b200 import expr as E
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    return (a * b).ge(c).and_(a.ne(0)), [E.ColType(38, 9)] * 3
+
+
+def run_filter(args, rank, world):
+    """A step is the WHERE clause of a query over 64M rows: the predicate
+    module writes one flag byte per row, then up_filter_flags writes the kept
+    rows' indices in row order (count, scan, ordered scatter)."""
+    import torch
+    from ultraprecise_b200 import runtime
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    hbm_peak, peak_kind = peaks()
+    rows = max(1, int((64 << 20) * args.rows_scale))
+    e, ct = filter_expr()
+    m = runtime.compile_expr(e, ct)
+    with torch.cuda.stream(stream):
+        cols = [runtime.gen_digits(rows, 38, 40 + 3 * rank + k, stream=stream) for k in range(3)]
+    torch.cuda.synchronize()
+    dc = [runtime.DeviceColumn(t, 38, 9) for t in cols]
+    flags = torch.empty(rows, dtype=torch.uint8, device="cuda")
+    idx = torch.empty(rows, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    from ultraprecise_b200 import abi
+    lib = abi.load()
+
+    def predicate():
+        m.launch(dc, rows, out=flags, stream=stream)
+
+    def select():
+        abi.check(lib.up_filter_flags(flags.data_ptr(), rows, idx.data_ptr(), cnt.data_ptr(), stream.cuda_stream),
+                  "up_filter_flags")
+
+    def timed(fn, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    def step():
+        predicate()
+        select()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    with ClockSampler(dev) as clk:
+        ms = max_over_ranks(timed(step, args.steps), world)
+    pred_ms = max_over_ranks(timed(predicate, args.steps), world)
+    sel_ms = max_over_ranks(timed(select, args.steps), world)
+    kept = int(cnt.item())
+    pred_bytes = 3 * 16 + 1
+    gbs = pred_bytes * rows / (pred_ms * 1e-3) / 1e9
+    sel_gbs = (rows + 4 * kept) / (sel_ms * 1e-3) / 1e9
+    res = {"metric": FILTER_METRIC, "value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
+           "config": {"workload": f"predicate + row selection over {rows} rows of 3 DECIMAL(38,9) columns, "
+                                  f"{kept} rows kept", "l2": "inputs larger than L2 (no flush)",
+                      "parallelism": f"replicas x{world} (no collective)"},
+           "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+                        "frac": round(gbs / hbm_peak, 4), "traffic": None, "kernel": "up_expr_tile (predicate)",
+                        "peak_source": peak_kind, "bytes_per_row": pred_bytes},
+           "predicate_ms": round(pred_ms, 4), "select_ms": round(sel_ms, 4),
+           "select_gbs": round(sel_gbs, 1), "gpu_launches": 4 * args.steps, "clocks": clk.summary()}
+    if not args.no_e2e:
+        pairs = []
+        for t in cols:
+            h = torch.empty(t.numel(), dtype=torch.uint8, pin_memory=True)
+            h.copy_(t)
+            pairs.append((t, h))
+        hidx = torch.empty(rows, dtype=torch.int32, pin_memory=True)
+
+        def e2e_step():
+            with torch.cuda.stream(stream):
+                for d, h in pairs:
+                    d.copy_(h, non_blocking=True)
+            step()
+            with torch.cuda.stream(stream):
+                hidx[:kept].copy_(idx[:kept], non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        n = max(1, min(args.steps, 3))
+        ems = max_over_ranks(timed(e2e_step, n), world)
+        res["e2e"] = {"value": round(rows * world / (ems * 1e-3)), "unit": "rows/s",
+                      "h2d_bytes_per_step": 3 * 16 * rows, "d2h_bytes_per_step": 4 * kept,
+                      "ms_per_step": round(ems, 3), "steps": n}
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        rate, srows = filter_cpu_rate(args.cpu_seconds, os.cpu_count() or 1)
+        res["cpu_baseline"] = {"value": round(rate), "unit": "rows/s", "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"{srows} rows of the same predicate and selection, oracle on "
+                                         f"{os.cpu_count() or 1} host threads"}
+    return res
+
+
 # ------------------------------------------------------ CPU baseline
 def cpu_rate(cases, cpu_seconds, threads, seed=1):
     """Time the oracle on the host cores over the same sweep mix (every case
@@ -1122,6 +1251,15 @@ def run_reference(args, rank, world):
                                                 "parallelism": f"{threads} host threads"},
                 "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
                                  "sample": sample},
+                "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "filter":
+        rate, rows = filter_cpu_rate(args.cpu_seconds, threads)
+        return {"metric": FILTER_METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u32 limbs (exact decimal)", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "predicate + row selection on host cores, bounded sample", "rows": rows},
+                "cpu_baseline": {"kind": "port", "cores": threads, "value": round(rate),
+                                 "sample": f"{rows} rows of the predicate and selection"},
                 "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "query":
         per = args.cpu_seconds / max(1, args.steps)
@@ -1210,7 +1348,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    run = {"batch": run_batch, "query": run_query, "sin": run_sin, "serve": run_serve, "text": run_text}.get(
+    run = {"batch": run_batch, "query": run_query, "sin": run_sin, "serve": run_serve, "text": run_text,
+           "filter": run_filter}.get(
         args.workload, run_ours)
     res = run(args, rank, world)
     if world > 1:

@@ -63,12 +63,16 @@ def test_and_or_cooperative_matches_oracle():
         assert err == exp_err
 
 
-@pytest.mark.parametrize("rows,density", [(1, 1.0), (4095, 0.5), (4096, 0.0), (4097, 1.0), (100_003, 0.3),
-                                          (5_000_000, 0.01), (5_000_000, 0.999)])
-def test_filter_flags_matches_nonzero(rows, density):
-    g = torch.Generator(device="cuda").manual_seed(rows)
-    flags = (torch.rand(rows, device="cuda", generator=g) < density).to(torch.uint8)
+@pytest.mark.parametrize("rows,density,offset", [(1, 1.0, 0), (4095, 0.5, 0), (4096, 0.0, 0), (4097, 1.0, 0),
+                                                 (100_003, 0.3, 0), (100_003, 0.3, 5), (5_000_000, 0.01, 0),
+                                                 (5_000_000, 0.999, 0), (70_000, 0.5, 3)])
+def test_filter_flags_matches_nonzero(rows, density, offset):
+    """Flag bytes of any nonzero value; an offset misaligns the flags, which
+    takes the byte-wise path."""
+    g = torch.Generator(device="cuda").manual_seed(rows + offset)
+    flags = (torch.rand(rows + offset, device="cuda", generator=g) < density).to(torch.uint8)
     flags[flags == 1] = torch.randint(1, 256, (int(flags.sum()),), device="cuda", dtype=torch.int32).to(torch.uint8)
+    flags = flags[offset:]
     idx = runtime.filter_flags(flags, rows)
     exp = np.nonzero(flags.cpu().numpy())[0].astype(np.int32)
     assert np.array_equal(idx.cpu().numpy(), exp)
