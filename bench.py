@@ -523,6 +523,7 @@ def cpu_baseline_batch(tasks, cpu_seconds):
 # ------------------------------------------------------------ query workload
 QUERY_METRIC = "decimal rows/s (fused grouped SUM/AVG/COUNT query over DECIMAL(15,2)), bit-exact"
 QUERY_BYTES_PER_ROW = 4 * 7 + 2  # four 7-byte decimal columns and two 1-byte keys
+QUERY_MAX_GROUPS = 64  # output capacity of the grouped query (2 CHAR(1) keys give 4 groups here)
 
 
 def query_inputs(rows, seed, stream=None):
@@ -545,7 +546,8 @@ def run_query(args, rank, world):
     """One step = the whole grouped query from the raw columns: the key table
     from the two CHAR(1) key columns (one pass over the key bytes), then the
     fused query kernel, which reads the key bytes itself and maps them through
-    the table (no group-id array)."""
+    the table (no group-id array).  The group count stays on the device (it
+    picks the accumulation mode there), so a step has no host round trip."""
     import torch
     from ultraprecise_b200 import abi, runtime, workloads
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -574,12 +576,12 @@ def run_query(args, rank, world):
             torch.cuda.synchronize()
             _, G, _ = runtime.group_table_from_keys([k1, k2], keyb, stream=stream, table=table)
         dc = [runtime.DeviceColumn(c, 15, 2) for c in cols]
-        outs = [torch.empty(G * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES), dtype=torch.uint8,
-                            device="cuda") for k, _ in aggs]
+        outs = [torch.empty(QUERY_MAX_GROUPS * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES),
+                            dtype=torch.uint8, device="cuda") for k, _ in aggs]
 
         def step():
-            _, g, _ = runtime.group_table_from_keys([k1, k2], keyb, stream=stream, table=table, distinct=False)
-            q.launch_keys(dc, [k1, k2], keyb, table, g, outs=outs, err=err, stream=stream)
+            runtime.group_table_from_keys_async([k1, k2], keyb, table, stream=stream)
+            q.launch_keys_async(dc, [k1, k2], keyb, table, QUERY_MAX_GROUPS, outs=outs, err=err, stream=stream)
 
         def kernel_only():
             q.launch_keys(dc, [k1, k2], keyb, table, G, outs=outs, err=err, stream=stream)
@@ -614,14 +616,14 @@ def run_query(args, rank, world):
            "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
            "config": {"workload": f"grouped SUMx4/AVGx3/COUNT query, DECIMAL(15,2) x4, 2 CHAR(1) keys, "
-                                  f"{m['rows']} rows, step = key table + fused query "
+                                  f"{m['rows']} rows, step = key table + fused query, no host round trip "
                                   f"(256M roofline run; 1M-row case in 'rows_1m')",
                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world} (no collective)"},
            "roofline": {"bound": "hbm", "achieved": m["hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
                         "frac": m["hbm_frac"], "traffic": None, "kernel": "up_query_tile_r (+ up_query_fin)",
                         "peak_source": peak_kind, "bytes_per_row": QUERY_BYTES_PER_ROW},
            "detail": {k: m[k] for k in ("query_kernel_ms", "two_pass_group_ids_ms", "groups")},
-           "rows_1m": results["1M"], "gpu_launches": 4 * args.steps, "clocks": m["clocks"]}
+           "rows_1m": results["1M"], "gpu_launches": 5 * args.steps, "clocks": m["clocks"]}
     if not args.no_e2e:
         res["e2e"] = e2e_query(args, q, aggs, inputs, world, stream)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
@@ -654,8 +656,8 @@ def e2e_query(args, q, aggs, inputs, world, stream):
         with torch.cuda.stream(stream):
             for d, h in pairs:
                 d.copy_(h, non_blocking=True)
-            _, g, _ = runtime.group_table_from_keys([k1, k2], [1, 1], stream=stream, table=table, distinct=False)
-            q.launch_keys(dc, [k1, k2], [1, 1], table, g, outs=outs, stream=stream)
+            runtime.group_table_from_keys_async([k1, k2], [1, 1], table, stream=stream)
+            q.launch_keys_async(dc, [k1, k2], [1, 1], table, QUERY_MAX_GROUPS, outs=outs, stream=stream)
             for h, o in zip(hout, outs):
                 h.copy_(o, non_blocking=True)
 

@@ -226,11 +226,12 @@ up_status up_group_ids_from_keys(const void* const* key_cols, const int32_t* key
 /* The grouping of up_group_ids_from_keys without the per-row id array: one
  * pass over the key bytes marks the keys present, and `key_table` (DEVICE
  * int32, UP_KEY_TABLE_ENTRIES entries) receives in entries [0, 65536) each
- * possible key's dense id in ascending key order (-1 where absent) and in
- * entries [65536, 65536 + n_groups) the key of each id.  A key is its bytes
- * in column order, most significant first.  Synchronises `stream` to return
- * *n_groups. */
-#define UP_KEY_TABLE_ENTRIES 131072
+ * possible key's dense id in ascending key order (-1 where absent), in
+ * entries [65536, 65536 + n_groups) the key of each id, and the group count
+ * in entry UP_KEY_TABLE_COUNT.  A key is its bytes in column order, most
+ * significant first.  Synchronises `stream` to return *n_groups. */
+#define UP_KEY_TABLE_ENTRIES 131088
+#define UP_KEY_TABLE_COUNT 131072 /* entry holding the group count */
 up_status up_group_table_from_keys(const void* const* key_cols, const int32_t* key_bytes,
                                    int32_t n_keys, int64_t rows, int32_t* key_table,
                                    int32_t* n_groups, void* group_keys, void* stream);
@@ -244,6 +245,20 @@ up_status up_query_launch_keys(up_module* query, const up_column* in, int32_t n_
                                const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
                                const int32_t* key_table, int32_t n_groups, void* const* outs,
                                uint32_t* err_word, void* stream);
+
+/* The same pair without a round trip to the host: the table call does not
+ * synchronise, and the query reads the group count from the table on the
+ * device, choosing its accumulation mode there.  Outputs are sized for
+ * `max_groups` groups (1..65536); a count above it sets UP_ROWERR_DOMAIN and
+ * leaves the outputs unwritten.  The group count is read back by the caller
+ * from entry UP_KEY_TABLE_COUNT when it needs it. */
+up_status up_group_table_from_keys_async(const void* const* key_cols, const int32_t* key_bytes,
+                                         int32_t n_keys, int64_t rows, int32_t* key_table,
+                                         void* group_keys, void* stream);
+up_status up_query_launch_keys_async(up_module* query, const up_column* in, int32_t n_in, int64_t rows,
+                                     const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                     const int32_t* key_table, int32_t max_groups, void* const* outs,
+                                     uint32_t* err_word, void* stream);
 
 /* ------------------------------------- fused expression + group aggregate */
 typedef struct up_query_agg {

@@ -156,3 +156,96 @@ def test_key_outside_the_table_is_a_domain_error(groups):
     q.launch_keys(dev, [k], [1], table, G, err=err)
     torch.cuda.synchronize()
     assert int(err.item()) & abi.UP_ROWERR_DOMAIN
+
+
+def _mode_query():
+    cols = [E.ColType(15, 2), E.ColType(30, 5), E.ColType(15, 2)]
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    exprs = [a, a * b, b - c, a * c + b]
+    aggs = [(abi.UP_AGG_SUM, 0), (abi.UP_AGG_SUM, 1), (abi.UP_AGG_AVG, 2), (abi.UP_AGG_COUNT, 0),
+            (abi.UP_AGG_AVG, 0), (abi.UP_AGG_SUM, 3)]
+    return runtime.compile_query(exprs, aggs, cols), cols
+
+
+@pytest.mark.parametrize("layout,groups,rows,offset,cap", [
+    ("2x1", 4, 1_000_000, 0, 4), ("2x1", 4, 100_000, 0, 64), ("1x1", 9, 20_000, 1, 256),
+    ("1x1", 200, 200_000, 0, 256), ("1x2", 5000, 300_000, 0, 8192), ("2x1", 3000, 7_777, 1, 65536)])
+def test_async_pair_matches_sync(layout, groups, rows, offset, cap):
+    """Key table and query without a host round trip (the group count stays on
+    the device and picks the accumulation mode there) give the same bytes as
+    the synchronous pair, whatever the output capacity."""
+    q, cols = _mode_query()
+    n = rows + offset
+    raw = [runtime.gen_digits(n, ct.precision, 5 * groups + i, signed=True) for i, ct in enumerate(cols)]
+    dev = [runtime.DeviceColumn(t[offset * codec.compact_bytes(ct.precision):], ct.precision, ct.scale)
+           for t, ct in zip(raw, cols)]
+    keys_all, kb = _make_keys(layout, groups, n, seed=groups + 11 * rows)
+    keys = [k[offset * w:] for k, w in zip(keys_all, kb)]
+    table, G, _ = runtime.group_table_from_keys(keys, kb)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    exp = q.launch_keys(dev, keys, kb, table, G, err=err, rows=rows)
+    table2 = torch.full((abi.UP_KEY_TABLE_ENTRIES,), -7, dtype=torch.int32, device="cuda")
+    runtime.group_table_from_keys_async(keys, kb, table2)
+    err2 = torch.zeros(1, dtype=torch.int32, device="cuda")
+    got = q.launch_keys_async(dev, keys, kb, table2, cap, err=err2, rows=rows)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0 and int(err2.item()) == 0
+    assert int(table2[abi.UP_KEY_TABLE_COUNT].item()) == G
+    assert torch.equal(table2[:65536 + G], table[:65536 + G])
+    for k, (o, e) in enumerate(zip(got, exp)):
+        assert torch.equal(o[: e.numel()], e), f"aggregate {k}"
+
+
+def test_async_count_above_capacity_is_a_domain_error():
+    q, cols = _mode_query()
+    rows = 10_000
+    raw = [runtime.gen_digits(rows, ct.precision, 3 + i) for i, ct in enumerate(cols)]
+    dev = [runtime.DeviceColumn(t, ct.precision, ct.scale) for t, ct in zip(raw, cols)]
+    keys, kb = _make_keys("1x1", 20, rows, seed=4)
+    table = torch.empty(abi.UP_KEY_TABLE_ENTRIES, dtype=torch.int32, device="cuda")
+    runtime.group_table_from_keys_async(keys, kb, table)
+    outs = [torch.full((8 * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES),), 0xAB, dtype=torch.uint8,
+                       device="cuda") for k, _ in q.aggs]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    q.launch_keys_async(dev, keys, kb, table, 8, outs=outs, err=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) & abi.UP_ROWERR_DOMAIN
+    assert all(bool((o == 0xAB).all()) for o in outs)
+
+
+def test_async_pair_replays_in_a_cuda_graph():
+    """The whole grouped query (key table + fused query) captured once and
+    replayed over new key and value data gives the synchronous pair's bytes."""
+    exprs, aggs, cols = config0_query()
+    q = runtime.compile_query(exprs, aggs, cols)
+    rows, cap = 200_000, 16
+    qty, price, disc, tax, k1, k2 = config0_columns(rows, 1)
+    dev = [runtime.DeviceColumn(t, 15, 2) for t in (qty, price, disc, tax)]
+    table = torch.empty(abi.UP_KEY_TABLE_ENTRIES, dtype=torch.int32, device="cuda")
+    outs = [torch.empty(cap * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES), dtype=torch.uint8,
+                        device="cuda") for k, _ in q.aggs]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):  # load the modules outside the capture
+        runtime.group_table_from_keys_async([k1, k2], [1, 1], table, stream=side)
+        q.launch_keys_async(dev, [k1, k2], [1, 1], table, cap, outs=outs, err=err, stream=side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        s = torch.cuda.current_stream()
+        runtime.group_table_from_keys_async([k1, k2], [1, 1], table, stream=s)
+        q.launch_keys_async(dev, [k1, k2], [1, 1], table, cap, outs=outs, err=err, stream=s)
+    for seed in (2, 3):
+        new = config0_columns(rows, seed)
+        for dst, src in zip((qty, price, disc, tax, k1, k2), new):
+            dst.copy_(src)
+        err.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        t2, G, _ = runtime.group_table_from_keys([k1, k2], [1, 1])
+        exp = q.launch_keys(dev, [k1, k2], [1, 1], t2, G)
+        torch.cuda.synchronize()
+        for k, (o, e) in enumerate(zip(outs, exp)):
+            assert torch.equal(o[: e.numel()], e), f"seed {seed} aggregate {k}"
+    del graph

@@ -41,7 +41,8 @@ UP_NODE_NE = 15
 UP_NODE_AND = 16
 UP_NODE_OR = 17
 UP_NODE_RESCALE = 20
-UP_KEY_TABLE_ENTRIES = 131072
+UP_KEY_TABLE_ENTRIES = 131088
+UP_KEY_TABLE_COUNT = 131072
 COMPARE_KINDS = (UP_NODE_LT, UP_NODE_LE, UP_NODE_GT, UP_NODE_GE, UP_NODE_EQ, UP_NODE_NE, UP_NODE_AND, UP_NODE_OR)
 
 UP_CONST_MAX_LIMBS = 128
@@ -128,6 +129,8 @@ SIGNATURES = {
     "up_expr_launch": (_I32, [_P, _P, _I32, _I64, _P, _P, _P]),
     "up_group_table_from_keys": (_I32, [_P, _P, _I32, _I64, _P, _PI32, _P, _P]),
     "up_query_launch_keys": (_I32, [_P, _P, _I32, _I64, _P, _P, _I32, _P, _I32, _P, _P, _P]),
+    "up_group_table_from_keys_async": (_I32, [_P, _P, _I32, _I64, _P, _P, _P]),
+    "up_query_launch_keys_async": (_I32, [_P, _P, _I32, _I64, _P, _P, _I32, _P, _I32, _P, _P, _P]),
     "up_filter_flags": (_I32, [_P, _I64, _P, _P, _P]),
     "up_parse_decimal": (_I32, [_P, _P, _I64, _I32, _I32, _P, _P, _P]),
     "up_format_width": (_I32, [_I32, _I32]),

@@ -362,6 +362,8 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
                           int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread,
                           const QueryKeys* keys) {
     if (!m || !m->is_query) return fail(UP_ERR_INVALID_ARG, "not a query module");
+    const bool device_count = keys && keys->capacity > 0;
+    if (device_count) n_groups = keys->capacity;  // accumulators and outputs sized for the capacity
     if (rows < 0 || n_groups < 0) return fail(UP_ERR_INVALID_ARG, "negative size");
     if (n_groups == 0) return UP_OK;
     if (rows > 0 && !keys && !group_ids) return fail(UP_ERR_INVALID_ARG, "group ids are NULL");
@@ -391,7 +393,7 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
     a.acc = (uint32_t*)scratch;
     a.cnt = (uint64_t*)((uint8_t*)scratch + acc_bytes);
     a.err = err_word;
-    a.n_groups = n_groups;
+    a.n_groups = device_count ? -n_groups : n_groups;
     a.vec_ok = vec_ok ? 1 : 0;
     bool keys_aligned = aligned16(group_ids);
     if (keys) {
@@ -407,19 +409,28 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
             // staged tiles; accumulators in registers, shared memory or global
             // memory by group count
             const bool reg = g.q_gr > 0 && n_groups <= g.q_gr;
-            const char* name = reg ? (keys ? "up_query_tile_rk" : "up_query_tile_r")
-                               : (n_groups <= g.q_gs) ? "up_query_tile_s"
-                                                      : "up_query_tile_g";
+            const char* reg_name = keys ? "up_query_tile_rk" : "up_query_tile_r";
+            const char* name = reg ? reg_name : (n_groups <= g.q_gs) ? "up_query_tile_s" : "up_query_tile_g";
             a.vec_ok = (vec_ok && keys_aligned) ? 1 : 0;
-            void* k = jit_kernel(*m->jm.ks, name);
-            st = set_smem(k, g.q_smem);  // the tile layout is kept within 48 KB: normally a no-op
-            if (st != UP_OK) return st;
             const int64_t ntiles = (rows + g.q_tile_rows - 1) / g.q_tile_rows;
-            // the register and shared-memory modes merge once per CTA, so a
-            // spread launch keeps a bounded grid of several waves
-            const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, g.q_smem) * (spread ? 8 : 1);
-            e = cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(ntiles, cap)), dim3(g.block_threads),
-                                 args, (size_t)g.q_smem, s);
+            auto launch_tile = [&](const char* kname) -> cudaError_t {
+                void* k = jit_kernel(*m->jm.ks, kname);
+                if (set_smem(k, g.q_smem) != UP_OK) return cudaErrorInvalidValue;  // layout kept within 48 KB
+                // the register and shared-memory modes merge once per CTA, so a
+                // spread launch keeps a bounded grid of several waves
+                const int64_t cap = (int64_t)sms * occupancy(k, g.block_threads, g.q_smem) * (spread ? 8 : 1);
+                return cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(ntiles, cap)),
+                                        dim3(g.block_threads), args, (size_t)g.q_smem, s);
+            };
+            if (device_count) {
+                // the mode follows the count on the device: every applicable
+                // mode kernel is launched and all but one return at once
+                if (g.q_gr > 0) e = launch_tile(reg_name);
+                if (e == cudaSuccess && (g.q_gr == 0 || n_groups > g.q_gr)) e = launch_tile("up_query_tile_s");
+                if (e == cudaSuccess && n_groups > g.q_gs) e = launch_tile("up_query_tile_g");
+            } else {
+                e = launch_tile(name);
+            }
         } else {
             void* k = jit_kernel(*m->jm.ks, "up_query_acc");
             const int64_t blocks = (rows + g.block_threads - 1) / g.block_threads;
@@ -536,12 +547,9 @@ up_status up_group_table_from_keys(const void* const* key_cols, const int32_t* k
     return UP_OK;
 }
 
-up_status up_query_launch_keys(up_module* m, const up_column* in, int32_t n_in, int64_t rows,
-                               const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
-                               const int32_t* key_table, int32_t n_groups, void* const* outs, uint32_t* err_word,
-                               void* stream) {
+static up_status query_keys_of(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                               const int32_t* key_table, int64_t rows, QueryKeys& k) {
     if (!key_cols || !key_bytes || !key_table) return fail(UP_ERR_INVALID_ARG, "NULL key arguments");
-    QueryKeys k;
     if (n_keys == 1 && key_bytes[0] == 1) k.mode = 1;
     else if (n_keys == 2 && key_bytes[0] == 1 && key_bytes[1] == 1) k.mode = 2;
     else if (n_keys == 1 && key_bytes[0] == 2) k.mode = 3;
@@ -550,7 +558,46 @@ up_status up_query_launch_keys(up_module* m, const up_column* in, int32_t n_in, 
     k.key1 = k.mode == 2 ? (const uint8_t*)key_cols[1] : nullptr;
     k.table = key_table;
     if (rows > 0 && (!k.key0 || (k.mode == 2 && !k.key1))) return fail(UP_ERR_INVALID_ARG, "key column is NULL");
+    return UP_OK;
+}
+
+up_status up_query_launch_keys(up_module* m, const up_column* in, int32_t n_in, int64_t rows,
+                               const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                               const int32_t* key_table, int32_t n_groups, void* const* outs, uint32_t* err_word,
+                               void* stream) {
+    QueryKeys k;
+    const up_status st = query_keys_of(key_cols, key_bytes, n_keys, key_table, rows, k);
+    if (st != UP_OK) return st;
     return query_launch_ex(m, in, n_in, rows, nullptr, n_groups, outs, err_word, stream, false, &k);
+}
+
+up_status up_query_launch_keys_async(up_module* m, const up_column* in, int32_t n_in, int64_t rows,
+                                     const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                     const int32_t* key_table, int32_t max_groups, void* const* outs,
+                                     uint32_t* err_word, void* stream) {
+    if (max_groups < 1 || max_groups > 65536) return fail(UP_ERR_INVALID_ARG, "max_groups must be 1..65536");
+    QueryKeys k;
+    const up_status st = query_keys_of(key_cols, key_bytes, n_keys, key_table, rows, k);
+    if (st != UP_OK) return st;
+    k.capacity = max_groups;
+    return query_launch_ex(m, in, n_in, rows, nullptr, max_groups, outs, err_word, stream, false, &k);
+}
+
+up_status up_group_table_from_keys_async(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                         int64_t rows, int32_t* key_table, void* group_keys, void* stream) {
+    if (!key_cols || !key_bytes || !key_table) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    if (rows < 0) return fail(UP_ERR_INVALID_ARG, "negative row count");
+    if (n_keys < 1 || n_keys > 4) return fail(UP_ERR_INVALID_ARG, "1..4 key columns");
+    int total = 0;
+    for (int k = 0; k < n_keys; k++) {
+        if (key_bytes[k] < 1) return fail(UP_ERR_INVALID_ARG, "key width < 1");
+        if (rows > 0 && !key_cols[k]) return fail(UP_ERR_INVALID_ARG, "key column is NULL");
+        total += key_bytes[k];
+    }
+    if (total > 2) return fail(UP_ERR_UNSUPPORTED, "direct key table supports at most 2 key bytes in total");
+    UP_CUDA(launch_group_table_small_keys_async(key_cols, key_bytes, n_keys, rows, key_table, group_keys,
+                                                (cudaStream_t)stream));
+    return UP_OK;
 }
 
 up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,

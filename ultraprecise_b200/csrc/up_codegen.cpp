@@ -277,6 +277,20 @@ UP_DI int q_tile_group(const UpQArgs& a, const u8* t, int r, int R) {
     if (a.key_mode == 0) return ((const int*)t)[r];
     return __ldg(a.key_table + q_tile_key(a, t, r, R));
 }
+// The group count: n_groups when it is >= 0; otherwise the count the key
+// table holds (entry 131072), with -n_groups the capacity of the
+// accumulators and outputs; -1 when the table's count exceeds it.
+UP_DI int q_groups(const UpQArgs& a) {
+    if (a.n_groups >= 0) return a.n_groups;
+    const int n = *(volatile const int*)(a.key_table + 131072);
+    return (n >= 0 && n <= -a.n_groups) ? n : -1;
+}
+// groups held in shared memory by a tile kernel of this mode (recomputed
+// where needed, so that no register holds it through the row loop)
+UP_DI int q_nsm(const UpQArgs& a, int mode, int gr) {
+    const int n = q_groups(a);
+    return mode == 0 ? (n < gr ? n : gr) : (mode == 1 ? n : 0);
+}
 )";
 }
 
@@ -911,10 +925,12 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     // generic kernel: blocks, indirection, nullable values; global accumulators
     src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_query_acc(const UpQArgs a) {\n";
     src << "    u32 err = 0u;\n";
+    src << "    const int ngr = q_groups(a);\n";
+    src << "    if (ngr < 0) { if (threadIdx.x == 0 && blockIdx.x == 0 && a.err) atomicOr(a.err, ERR_DOMAIN); return; }\n";
     src << "    const i64 stride = (i64)gridDim.x * blockDim.x;\n";
     src << "    for (i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x; row < a.rows; row += stride) {\n";
     src << "        const int g = q_group(a, row);\n";
-    src << "        if ((unsigned)g >= (unsigned)a.n_groups) { err |= ERR_DOMAIN; continue; }\n";
+    src << "        if ((unsigned)g >= (unsigned)ngr) { err |= ERR_DOMAIN; continue; }\n";
     src << "        atomicAdd(a.cnt + g, 1ull);\n";
     src << "        bool isnull = false;\n";
     for (int c : used) {
@@ -988,7 +1004,12 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         src << "    u64* bar = (u64*)(sm + " << off_bar << ");\n";
         src << "    u32* sacc = (u32*)(sm + " << off_acc << ");\n";
         src << "    u32* scnt = (u32*)(sm + " << off_cnt << ");\n";
-        src << "    const int ng = a.n_groups;\n";
+        // the launch picks the mode by group count; with the count on the
+        // device every mode is launched and all but one return here
+        src << "    const int ng = q_groups(a);\n";
+        src << "    if (ng < 0) { if (threadIdx.x == 0 && blockIdx.x == 0 && a.err) atomicOr(a.err, ERR_DOMAIN); return; }\n";
+        src << "    if (MODE == 0 ? ng > " << GR << " : MODE == 1 ? ((" << GR << " > 0 && ng <= " << GR << ") || ng > " << GS
+            << ") : ng <= " << GS << ") return;\n";
         src << "    const int nsm = MODE == 0 ? (ng < GR ? ng : GR) : (MODE == 1 ? ng : 0);\n";
         src << "    for (int i = threadIdx.x; i < nsm * W; i += blockDim.x) sacc[i] = 0u;\n";
         src << "    for (int i = threadIdx.x; i < nsm; i += blockDim.x) scnt[i] = 0u;\n";
@@ -1078,7 +1099,8 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
                 src << "                const bool f" << i << " = fits_twos64(qv" << i << ");\n";
                 src << "                if (!f" << i << ") {  // rare: wider than 64 bits\n";
                 src << "                    const int gw = KEYS ? __ldg(a.key_table + key) : g;\n";
-                src << "                    if ((unsigned)gw < (unsigned)nsm) atomic_add_twos(sacc + gw * W + " << acc_off[i]
+                src << "                    if ((unsigned)gw < (unsigned)q_nsm(a, MODE, GR)) atomic_add_twos(sacc + gw * W + "
+                    << acc_off[i]
                     << ", qv" << i << ");\n                }\n";
             }
         src << "#pragma unroll\n                for (int j = 0; j < GR; j++)\n";
@@ -1127,7 +1149,8 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         src << "    }\n";
         src << "    if constexpr (MODE != 2) {\n";
         src << "        __syncthreads();\n";
-        src << "        for (int gg = threadIdx.x; gg < nsm; gg += blockDim.x) {\n";
+        src << "        const int nsm_end = q_nsm(a, MODE, GR);\n";
+        src << "        for (int gg = threadIdx.x; gg < nsm_end; gg += blockDim.x) {\n";
         src << "            const u32 c = scnt[gg];\n";
         src << "            if (c == 0u) continue;\n";
         src << "            atomicAdd(a.cnt + gg, (u64)c);\n";
@@ -1157,7 +1180,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
 
     src << "extern \"C\" __global__ void __launch_bounds__(256) up_query_fin(const UpQArgs a) {\n";
     src << "    const int g = blockIdx.x * blockDim.x + threadIdx.x;\n";
-    src << "    if (g >= a.n_groups) return;\n";
+    src << "    if (g >= q_groups(a)) return;\n";
     src << "    const u64 cnt = a.cnt[g];\n";
     src << "    const u32* acc = a.acc + (i64)g * " << std::max(accw, 1) << ";\n";
     src << "    const u32 P10_4[1] = {10000u};\n";

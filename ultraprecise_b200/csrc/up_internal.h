@@ -196,6 +196,9 @@ struct QueryKeys {
     const uint8_t* key1 = nullptr;
     const int32_t* table = nullptr;
     int mode = 0;
+    // > 0: the group count is read on the device from the key table (entry
+    // 131072) and may be at most `capacity`, which sizes the accumulators
+    int capacity = 0;
 };
 up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
                           int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread,

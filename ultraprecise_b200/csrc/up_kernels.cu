@@ -79,7 +79,8 @@ cudaError_t launch_division_int64(const uint8_t* sums, const int64_t* counts, in
 // order, most significant first, so ascending keys are the order of the
 // reference's sort-based GroupColumns (AriesSqlOperator_group.cu:14-54).
 // The key table maps each of the 65536 possible keys to its dense group id
-// (-1 for an absent key); its second half lists the present keys by id.
+// (-1 for an absent key); its second half lists the present keys by id, and
+// entry 131072 holds the group count.
 struct KeyCols {
     const u8* col[4];
     int bytes[4];
@@ -227,20 +228,31 @@ cudaError_t group_table_async(const KeyCols& k, int total, int64_t rows, int32_t
 
 }  // namespace
 
-cudaError_t launch_group_table_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
-                                          int64_t rows, int32_t* table, int32_t* n_groups, void* group_keys,
-                                          cudaStream_t s) {
+// The key table: kTableKeys forward entries (key -> id), kTableKeys entries
+// of the id -> key list, then the group count at entry kTableCount.
+constexpr int kTableKeys = 65536;
+constexpr int kTableCount = 2 * kTableKeys;
+constexpr int kTableEntries = kTableCount + 16;
+
+cudaError_t launch_group_table_small_keys_async(const void* const* key_cols, const int32_t* key_bytes,
+                                                int32_t n_keys, int64_t rows, int32_t* table, void* group_keys,
+                                                cudaStream_t s) {
     int total = 0;
     const KeyCols k = key_cols_of(key_cols, key_bytes, n_keys, &total);
     void* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, kKeyWords * 4 + 16, s);
+    cudaError_t e = cudaMallocAsync(&scratch, kKeyWords * 4, s);
     if (e != cudaSuccess) return e;
-    u32* bits = (u32*)scratch;
-    int32_t* dn = (int32_t*)((u8*)scratch + kKeyWords * 4);
-    e = group_table_async(k, total, rows, table, dn, bits, group_keys, s);
+    e = group_table_async(k, total, rows, table, table + kTableCount, (u32*)scratch, group_keys, s);
+    const cudaError_t e2 = cudaFreeAsync(scratch, s);
+    return e != cudaSuccess ? e : e2;
+}
+
+cudaError_t launch_group_table_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
+                                          int64_t rows, int32_t* table, int32_t* n_groups, void* group_keys,
+                                          cudaStream_t s) {
+    cudaError_t e = launch_group_table_small_keys_async(key_cols, key_bytes, n_keys, rows, table, group_keys, s);
     int32_t hn = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&hn, dn, 4, cudaMemcpyDeviceToHost, s);
-    cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hn, table + kTableCount, 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e == cudaSuccess) *n_groups = hn;
     return e;
@@ -252,11 +264,12 @@ cudaError_t launch_group_ids_small_keys(const void* const* key_cols, const int32
     int total = 0;
     const KeyCols k = key_cols_of(key_cols, key_bytes, n_keys, &total);
     void* scratch = nullptr;
-    cudaError_t e = cudaMallocAsync(&scratch, 65536 * 4 + kKeyWords * 4 + 16, s);
+    // a whole key table (forward entries, id -> key list, count), then the bitmap
+    cudaError_t e = cudaMallocAsync(&scratch, (size_t)kTableEntries * 4 + kKeyWords * 4, s);
     if (e != cudaSuccess) return e;
     int32_t* table = (int32_t*)scratch;
-    u32* bits = (u32*)((u8*)scratch + 65536 * 4);
-    int32_t* dn = (int32_t*)((u8*)scratch + 65536 * 4 + kKeyWords * 4);
+    u32* bits = (u32*)((u8*)scratch + (size_t)kTableEntries * 4);
+    int32_t* dn = table + kTableCount;
     e = group_table_async(k, total, rows, table, dn, bits, group_keys, s);
     if (e == cudaSuccess && rows > 0) {
         const int sms = std::max(1, sm_count_current());

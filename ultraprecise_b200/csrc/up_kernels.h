@@ -15,7 +15,11 @@ cudaError_t launch_division_int64(const uint8_t* sums, const int64_t* counts, in
 cudaError_t launch_group_ids_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
                                         int64_t rows, int32_t* gid, int32_t* n_groups, void* group_keys,
                                         cudaStream_t s);
-// The 65536-entry key table only (no per-row ids); also synchronises.
+// The key table only (no per-row ids; UP_KEY_TABLE_ENTRIES entries, the
+// group count at entry 131072); the _async form does not synchronise.
+cudaError_t launch_group_table_small_keys_async(const void* const* key_cols, const int32_t* key_bytes,
+                                                int32_t n_keys, int64_t rows, int32_t* table, void* group_keys,
+                                                cudaStream_t s);
 cudaError_t launch_group_table_small_keys(const void* const* key_cols, const int32_t* key_bytes, int32_t n_keys,
                                           int64_t rows, int32_t* table, int32_t* n_groups, void* group_keys,
                                           cudaStream_t s);

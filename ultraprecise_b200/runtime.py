@@ -189,6 +189,29 @@ class QueryModule:
                                            _stream_ptr(stream)), "up_query_launch_keys")
         return list(outs)
 
+    def launch_keys_async(self, cols: Sequence[DeviceColumn], keys: Sequence[torch.Tensor],
+                          key_bytes: Sequence[int], key_table: torch.Tensor, max_groups: int,
+                          outs: Sequence[torch.Tensor] | None = None, err: torch.Tensor | None = None,
+                          stream=None, rows: int | None = None) -> list[torch.Tensor]:
+        """The query over key columns with the group count read on the device
+        from the key table (up_query_launch_keys_async): no host round trip.
+        Outputs hold `max_groups` groups, the first n_groups of them written."""
+        lib = abi.load()
+        if rows is None:
+            rows = keys[0].numel() // key_bytes[0]
+        if outs is None:
+            outs = [torch.empty(max_groups * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES),
+                                dtype=torch.uint8, device="cuda") for k, _ in self.aggs]
+        optr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+        arr = _columns_array(cols)
+        kp = (C.c_void_p * len(keys))(*[k.data_ptr() for k in keys])
+        kb = (C.c_int32 * len(keys))(*key_bytes)
+        abi.check(lib.up_query_launch_keys_async(self._h, arr, len(cols), rows, kp, kb, len(keys),
+                                                 key_table.data_ptr(), max_groups, optr,
+                                                 err.data_ptr() if err is not None else None, _stream_ptr(stream)),
+                  "up_query_launch_keys_async")
+        return list(outs)
+
     def __del__(self):
         try:
             abi.load().up_module_release(self._h)
@@ -265,6 +288,19 @@ def group_table_from_keys(keys: Sequence[torch.Tensor], key_bytes: Sequence[int]
                                            gkeys.data_ptr() if distinct else None, _stream_ptr(stream)),
               "up_group_table_from_keys")
     return table, n.value, (gkeys[: n.value * total] if distinct else None)
+
+
+def group_table_from_keys_async(keys: Sequence[torch.Tensor], key_bytes: Sequence[int], table: torch.Tensor,
+                                stream=None) -> torch.Tensor:
+    """The key table without synchronising (up_group_table_from_keys_async);
+    the group count stays on the device at table[UP_KEY_TABLE_COUNT]."""
+    lib = abi.load()
+    rows = keys[0].numel() // key_bytes[0]
+    kp = (C.c_void_p * len(keys))(*[k.data_ptr() for k in keys])
+    kb = (C.c_int32 * len(keys))(*key_bytes)
+    abi.check(lib.up_group_table_from_keys_async(kp, kb, len(keys), rows, table.data_ptr(), None,
+                                                 _stream_ptr(stream)), "up_group_table_from_keys_async")
+    return table
 
 
 def _text_buffers(fields: Sequence[bytes]):
