@@ -402,6 +402,18 @@ def run_batch(args, rank, world):
     torch.cuda.synchronize()
     same = all(torch.equal(a, c) for a, c in zip(outs, plain_out))
 
+    # the same loop waiting for each query before the next, as a launcher that
+    # synchronises after every kernel does (the reference's CallKernel)
+    def plain_sync_step():
+        for k, (t, m) in enumerate(zip(tasks, plain)):
+            if t["agg"] < 0:
+                m.launch(devcols[k], data[k][0], out=plain_out[k], err=err, stream=stream)
+            else:
+                m.launch(devcols[k], gids[k], t["groups"], outs=[plain_out[k]], err=err, stream=stream)
+            stream.synchronize()
+
+    ms_plain_sync = timed(plain_sync_step, max(1, min(args.steps, 3)), 1)
+
     rows = sum(t["rows"] for t in tasks)
     bytes_step = sum(t["rows"] * (t["in_bytes_per_row"] + t["out_bytes_per_row"]) for t in tasks)
     madds_step = sum(t["rows"] * t["madds_per_row"] for t in tasks)
@@ -420,6 +432,9 @@ def run_batch(args, rank, world):
            "rows_per_s": round(rows * world / (ms_batch * 1e-3)),
            "plain": {"ms_per_step": round(ms_plain, 4), "queries_per_s": round(n * world / (ms_plain * 1e-3), 2),
                      "speedup_batched": round(ms_plain / ms_batch, 3), "byte_equal": same},
+           "plain_synchronised": {"ms_per_step": round(ms_plain_sync, 4),
+                                  "queries_per_s": round(n * world / (ms_plain_sync * 1e-3), 2),
+                                  "speedup_batched": round(ms_plain_sync / ms_batch, 3)},
            "roofline": {"bound": "int32", "achieved": round(gmadds, 1), "peak": round(madd_peak.value / 1e9, 1),
                         "unit": "G limb-madd/s", "frac": round(gmadds * 1e9 / madd_peak.value, 4),
                         "traffic": None, "kernel": "up_batch band kernels (whole graph)",
