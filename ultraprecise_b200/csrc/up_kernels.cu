@@ -152,14 +152,19 @@ __global__ void __launch_bounds__(256) k_mark_keys(KeyCols k, int64_t rows, u32*
         if (sb[i]) atomicOr(&bits[i], sb[i]);
 }
 
-// one block: dense ids in key order from the presence bitmap (64 keys per
-// thread), the key table, the group count and the distinct keys
+// one block: dense ids in key order from the presence bitmap, the key table,
+// the group count and the distinct keys.  The bitmap and the exclusive count
+// before each 64-key range are staged in shared memory, then thread t writes
+// the table entries of keys t, t + 1024, ... (coalesced).
 __global__ void __launch_bounds__(1024) k_scan_keys(const u32* __restrict__ bits, int32_t* __restrict__ table,
                                                     int32_t* __restrict__ n_out, u8* __restrict__ keys_out,
                                                     int key_bytes) {
+    __shared__ u32 sbits[kKeyWords];
     __shared__ int part[1024];
     const int t = threadIdx.x;
     const u32 w0 = bits[2 * t], w1 = bits[2 * t + 1];
+    sbits[2 * t] = w0;
+    sbits[2 * t + 1] = w1;
     const int c = __popc(w0) + __popc(w1);
     part[t] = c;
     __syncthreads();
@@ -169,22 +174,28 @@ __global__ void __launch_bounds__(1024) k_scan_keys(const u32* __restrict__ bits
         part[t] += v;
         __syncthreads();
     }
-    int base = part[t] - c;
-    for (int j = 0; j < 64; j++) {
-        const int key = t * 64 + j;
-        const bool present = (((j < 32 ? w0 : w1) >> (j & 31)) & 1u) != 0u;
+    const int total = part[1023];
+    __syncthreads();
+    part[t] -= c;  // exclusive count before range t
+    __syncthreads();
+    for (int i = 0; i < 64; i++) {
+        const int key = i * 1024 + t;
+        const int range = key >> 6, b = key & 63;
+        const u32 lo = sbits[2 * range], hi = sbits[2 * range + 1];
+        const u32 wb = b < 32 ? lo : hi;
+        const bool present = ((wb >> (b & 31)) & 1u) != 0u;
+        int id = -1;
         if (present) {
-            table[key] = base;
-            table[65536 + base] = key;
+            const u32 below = (1u << (b & 31)) - 1u;
+            id = part[range] + (b < 32 ? __popc(lo & below) : __popc(lo) + __popc(hi & below));
+            table[65536 + id] = key;
             if (keys_out)
-                for (int b = 0; b < key_bytes; b++)
-                    keys_out[(int64_t)base * key_bytes + b] = (u8)(key >> (8 * (key_bytes - 1 - b)));
-            base++;
-        } else {
-            table[key] = -1;
+                for (int k = 0; k < key_bytes; k++)
+                    keys_out[(int64_t)id * key_bytes + k] = (u8)(key >> (8 * (key_bytes - 1 - k)));
         }
+        table[key] = id;
     }
-    if (t == 1023) *n_out = part[1023];
+    if (t == 0) *n_out = total;
 }
 
 __global__ void k_map_keys(KeyCols k, int64_t rows, const int32_t* __restrict__ table, int32_t* __restrict__ gid) {
