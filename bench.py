@@ -610,6 +610,18 @@ def run_query(args, rank, world):
             ms = max_over_ranks(timed(step, steps), world)
         # the fused query kernel alone (table fixed): the roofline figure
         kms = max_over_ranks(timed(kernel_only, steps), world)
+        # the same step captured once in a CUDA graph and replayed
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            step()
+        def replay():
+            with torch.cuda.stream(stream):  # replays on the current stream, the one timed
+                graph.replay()
+
+        replay()
+        torch.cuda.synchronize()
+        graph_ms = max_over_ranks(timed(replay, steps), world)
+        del graph
         # the two-pass pipeline for comparison: group-id array, then the query over it
         with torch.cuda.stream(stream):
             gid, _, _ = runtime.group_ids_from_keys([k1, k2], keyb, stream=stream)
@@ -620,7 +632,8 @@ def run_query(args, rank, world):
         results[label] = {"rows": rows, "groups": G, "ms_per_step": round(ms, 4),
                           "rows_per_s": round(rows * world / (ms * 1e-3)), "query_kernel_ms": round(kms, 4),
                           "hbm_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
-                          "two_pass_group_ids_ms": round(ids_ms, 4), "clocks": clk.summary()}
+                          "two_pass_group_ids_ms": round(ids_ms, 4), "graph_replay_ms": round(graph_ms, 4),
+                          "clocks": clk.summary()}
         if label == "256M":
             main = results[label]
             inputs = (cols, k1, k2, table, G, outs)
@@ -637,7 +650,7 @@ def run_query(args, rank, world):
            "roofline": {"bound": "hbm", "achieved": m["hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
                         "frac": m["hbm_frac"], "traffic": None, "kernel": "up_query_tile_r (+ up_query_fin)",
                         "peak_source": peak_kind, "bytes_per_row": QUERY_BYTES_PER_ROW},
-           "detail": {k: m[k] for k in ("query_kernel_ms", "two_pass_group_ids_ms", "groups")},
+           "detail": {k: m[k] for k in ("query_kernel_ms", "two_pass_group_ids_ms", "graph_replay_ms", "groups")},
            "rows_1m": results["1M"], "gpu_launches": 5 * args.steps, "clocks": m["clocks"]}
     if not args.no_e2e:
         res["e2e"] = e2e_query(args, q, aggs, inputs, world, stream)
