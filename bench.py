@@ -248,7 +248,7 @@ def run_ours(args, rank, world):
     res = {"metric": METRIC, "value": round(value), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-           "config": {"workload": "precision sweep (configs[1]): a*b+c and a/b on DECIMAL(p,p/4), "
+           "config": {"workload": "precision sweep: a*b+c and a/b on DECIMAL(p,p/4), "
                                   "p in 18,38,76,150,300,600; 16M rows p<=38 halved per doubling",
                       "rows_per_step_per_gpu": rows_per_step, "l2": "inputs larger than L2 (no flush)",
                       "parallelism": f"replicas x{world} (row shards, no collective)"},
@@ -1338,7 +1338,7 @@ def run_reference(args, rank, world):
             "warmup": args.warmup, "ms_per_step": round(total_rows / rate * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "precision sweep (configs[1]) on host cores, bounded sample",
+            "config": {"workload": "precision sweep on host cores, bounded sample",
                        "parallelism": f"{threads} host threads"},
             "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
                              "sample": f"{rows} rows per step: every sweep case at {frac:.2e} of its rows"},

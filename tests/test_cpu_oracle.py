@@ -137,7 +137,7 @@ def test_oracle_group_agg_matches_python():
 
 
 def test_tables_match_reference_values():
-    # values quoted from src/datatypes/decimal.cu:92 at the configs' precisions
+    # values quoted from src/datatypes/decimal.cu:92 at the workloads' precisions
     lib = abi.load()
     o = oracle.load()
     for p, b in [(15, 7), (16, 7), (18, 8), (31, 14), (37, 16), (38, 16), (47, 20), (76, 32), (77, 33), (100, 42),

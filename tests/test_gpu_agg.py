@@ -16,8 +16,8 @@ pytestmark = pytest.mark.gpu
 KEYS = [(b"A", b"F", 0.25), (b"N", b"F", 0.007), (b"N", b"O", 0.493), (b"R", b"F", 0.25)]
 
 
-def config0_columns(rows: int, seed: int):
-    """qty 1-50, price 900.00-104949.50, disc 0.00-0.10,
+def grouped_query_columns(rows: int, seed: int):
+    """The grouped-query columns: qty 1-50, price 900.00-104949.50, disc 0.00-0.10,
     tax 0.00-0.08, all DECIMAL(15,2); two CHAR(1) keys with the Q1 weights."""
     qty = runtime.gen_range(rows, 15, 100, 5000, 100, seed + 1)
     price = runtime.gen_range(rows, 15, 90000, 10494950, 1, seed + 2)
@@ -31,7 +31,7 @@ def config0_columns(rows: int, seed: int):
     return qty, price, disc, tax, k1.contiguous(), k2.contiguous()
 
 
-def config0_query():
+def grouped_query():
     cols = [E.ColType(15, 2)] * 4
     qty, price, disc, tax = [E.col(i) for i in range(4)]
     disc_price = price * (E.dec("1.00") - disc)
@@ -43,10 +43,10 @@ def config0_query():
 
 
 @pytest.mark.parametrize("rows", [1, 1000, 100_003, 1_000_000])
-def test_config0_fused_query_parity(rows):
-    qty, price, disc, tax, k1, k2 = config0_columns(rows, 20261203)
+def test_grouped_query_fused_parity(rows):
+    qty, price, disc, tax, k1, k2 = grouped_query_columns(rows, 20261203)
     gid, G, gkeys = runtime.group_ids_from_keys([k1, k2], [1, 1])
-    exprs, aggs, cols = config0_query()
+    exprs, aggs, cols = grouped_query()
     q = runtime.compile_query(exprs, aggs, cols)
     dev = [runtime.DeviceColumn(t, 15, 2) for t in (qty, price, disc, tax)]
     err = torch.zeros(1, dtype=torch.int32, device="cuda")

@@ -30,7 +30,7 @@ def _check(mod, cols_t, raws, rows, expr_root_built=None, err_expected=None):
     return got
 
 
-# element-wise a*b+c and a/b on DECIMAL(p, p/4), every digit
+# The precision sweep: element-wise a*b+c and a/b on DECIMAL(p, p/4), every digit
 # uniform 0-9, signs +/-, zero divisors redrawn (small row counts here; the
 # full sizes run in bench.py)
 @pytest.mark.parametrize("p", [18, 38, 76, 150, 300, 600])

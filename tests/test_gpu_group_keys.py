@@ -11,7 +11,7 @@ torch = pytest.importorskip("torch")
 from oracle import oracle
 from ultraprecise_b200 import abi, codec, runtime
 from ultraprecise_b200 import expr as E
-from tests.test_gpu_agg import config0_columns, config0_query
+from tests.test_gpu_agg import grouped_query_columns, grouped_query
 
 pytestmark = pytest.mark.gpu
 
@@ -71,9 +71,9 @@ def test_key_table_matches_numpy(layout, groups, rows, offset):
 
 
 @pytest.mark.parametrize("rows", [1, 1000, 100_003, 1_000_000])
-def test_config0_query_from_keys_matches_oracle(rows):
-    qty, price, disc, tax, k1, k2 = config0_columns(rows, 20261203)
-    exprs, aggs, cols = config0_query()
+def test_grouped_query_from_keys_matches_oracle(rows):
+    qty, price, disc, tax, k1, k2 = grouped_query_columns(rows, 20261203)
+    exprs, aggs, cols = grouped_query()
     q = runtime.compile_query(exprs, aggs, cols)
     table, G, _ = runtime.group_table_from_keys([k1, k2], [1, 1])
     dev = [runtime.DeviceColumn(t, 15, 2) for t in (qty, price, disc, tax)]
@@ -122,7 +122,7 @@ def test_query_from_keys_every_mode(layout, groups, rows, offset):
 
 def test_key_launch_rejects_bad_layouts():
     lib = abi.load()
-    exprs, aggs, cols = config0_query()
+    exprs, aggs, cols = grouped_query()
     q = runtime.compile_query(exprs, aggs, cols)
     k = torch.zeros(16, dtype=torch.uint8, device="cuda")
     table = torch.zeros(abi.UP_KEY_TABLE_ENTRIES, dtype=torch.int32, device="cuda")
@@ -143,10 +143,10 @@ def test_key_outside_the_table_is_a_domain_error(groups):
     """A table built from other rows than the launch's: rows whose key it
     lacks are flagged (register mode by the match count, the other modes by
     the table's -1)."""
-    exprs, aggs, cols = config0_query()
+    exprs, aggs, cols = grouped_query()
     q = runtime.compile_query(exprs, aggs, cols)
     rows = 50_000
-    qty, price, disc, tax, _, _ = config0_columns(rows, 5)
+    qty, price, disc, tax, _, _ = grouped_query_columns(rows, 5)
     k = (torch.arange(rows, device="cuda") % groups).to(torch.uint8)
     k[rows // 2:] = torch.where(k[rows // 2:] == 0, torch.full_like(k[rows // 2:], 200), k[rows // 2:])
     table, G, _ = runtime.group_table_from_keys([k[: rows // 2].contiguous()], [1])
@@ -216,10 +216,10 @@ def test_async_count_above_capacity_is_a_domain_error():
 def test_async_pair_replays_in_a_cuda_graph():
     """The whole grouped query (key table + fused query) captured once and
     replayed over new key and value data gives the synchronous pair's bytes."""
-    exprs, aggs, cols = config0_query()
+    exprs, aggs, cols = grouped_query()
     q = runtime.compile_query(exprs, aggs, cols)
     rows, cap = 200_000, 16
-    qty, price, disc, tax, k1, k2 = config0_columns(rows, 1)
+    qty, price, disc, tax, k1, k2 = grouped_query_columns(rows, 1)
     dev = [runtime.DeviceColumn(t, 15, 2) for t in (qty, price, disc, tax)]
     table = torch.empty(abi.UP_KEY_TABLE_ENTRIES, dtype=torch.int32, device="cuda")
     outs = [torch.empty(cap * (8 if k == abi.UP_AGG_COUNT else abi.UP_AGG_DECIMAL_BYTES), dtype=torch.uint8,
@@ -236,7 +236,7 @@ def test_async_pair_replays_in_a_cuda_graph():
         runtime.group_table_from_keys_async([k1, k2], [1, 1], table, stream=s)
         q.launch_keys_async(dev, [k1, k2], [1, 1], table, cap, outs=outs, err=err, stream=s)
     for seed in (2, 3):
-        new = config0_columns(rows, seed)
+        new = grouped_query_columns(rows, seed)
         for dst, src in zip((qty, price, disc, tax, k1, k2), new):
             dst.copy_(src)
         err.zero_()
