@@ -118,3 +118,77 @@ def division_int64(sum_img: bytes, count: int) -> bytes:
     s = (C.c_char * len(sum_img)).from_buffer_copy(sum_img)
     lib.orc_division_int64(s, count, out)
     return bytes(out)
+
+
+def compact_bytes(p: int) -> int:
+    """B(p) from the oracle's own table (the reference's byte table,
+    decimal.cu:92, with the p >= 300 extension)."""
+    b = load().orc_compact_bytes(p)
+    if b < 1:
+        raise ValueError(f"precision {p} out of range")
+    return b
+
+
+def _type_binary(kind: int, p1: int, s1: int, p2: int, s2: int) -> tuple[int, int]:
+    """Result (precision, scale) of one operator node, ListToBinTree's rules
+    (AriesEngineShell.cpp:115-141): ADD/SUB take the wider integer part plus a
+    carry digit over the larger scale; MUL adds integer digits and scales; DIV
+    (DIV_FIX_EX_FRAC = 4) is p1 - p2 + s2 + 4 + 1 over s1 + 4; MOD keeps the
+    divisor's precision at scale 0.  A DIV precision that would not exceed its
+    scale is widened to scale + 1 (the reference's uint16 fields wrap there)."""
+    if kind in (abi.UP_NODE_ADD, abi.UP_NODE_SUB):
+        s = max(s1, s2)
+        return max(p1 - s1, p2 - s2) + 1 + s, s
+    if kind == abi.UP_NODE_MUL:
+        return (p1 - s1) + (p2 - s2) + s1 + s2, s1 + s2
+    if kind == abi.UP_NODE_DIV:
+        p, s = p1 - p2 + s2 + 5, s1 + 4
+        return (p if p > s else s + 1), s
+    if kind == abi.UP_NODE_MOD:
+        return p2, 0
+    raise ValueError(f"node kind {kind} has no binary typing rule")
+
+
+def derive_types(built, root: int | None = None):
+    """Fill every inner node's (precision, scale) in place, children first,
+    with the reference's typing rules; the oracle's restatement of the
+    library's up_expr_derive_types, so that CPU-only callers (the reference
+    arm of the benchmark) never load the product library.  Integer literals
+    type as Decimal(int32_t) / Decimal(int64_t) do (decimal.cu:291-309):
+    precision 10 or 19, scale 0; comparisons and AND/OR give (1, 0); constants
+    and RESCALE nodes keep the type they were given."""
+    nodes = built.nodes
+    roots = [root] if root is not None else list(built.roots)
+    done: set[int] = set()
+
+    def visit(k: int) -> None:
+        stack = [(k, False)]
+        while stack:
+            i, expanded = stack.pop()
+            if i in done:
+                continue
+            nd = nodes[i]
+            if not expanded:
+                stack.append((i, True))
+                for ch in (nd.left, nd.right):
+                    if ch >= 0 and ch not in done:
+                        stack.append((ch, False))
+                continue
+            if nd.kind == abi.UP_NODE_COLUMN:
+                ct = built.col_types[nd.column]
+                nd.precision, nd.scale = ct.precision, ct.scale
+            elif nd.kind == abi.UP_NODE_INT:
+                fits32 = -2147483648 <= nd.int_value <= 2147483647
+                nd.precision, nd.scale = (10 if fits32 else 19), 0
+            elif nd.kind in (abi.UP_NODE_CONST, abi.UP_NODE_RESCALE):
+                pass
+            elif nd.kind in abi.COMPARE_KINDS:
+                nd.precision, nd.scale = 1, 0
+            else:
+                a, b = nodes[nd.left], nodes[nd.right]
+                nd.precision, nd.scale = _type_binary(nd.kind, a.precision, a.scale, b.precision, b.scale)
+            done.add(i)
+
+    for r in roots:
+        visit(r)
+    return built

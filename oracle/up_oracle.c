@@ -489,9 +489,11 @@ typedef struct {
     const up_col_type* col_types;
     const uint8_t* const* cols;
     orc_dec* vals;
-    uint8_t* done;
+    uint8_t* done;   /* 0 not yet evaluated, 1 a value, 2 NULL */
     uint32_t err;
 } eval_ctx;
+
+enum { EV_VALUE = 1, EV_NULL = 2 };
 
 /* boolean nodes: comparisons, and AND/OR of booleans (AEExprAndOrNode,
  * AriesExprCalcNode.cpp:667-760; non-null values only) */
@@ -502,17 +504,37 @@ static int col_value_bytes(const up_col_type* t) {
 }
 
 /* returns 0 on success, -1 on a malformed tree */
+/* NULL propagates: a nullable column's value is NULL when its flag byte
+ * (the leading byte of nullable_type, aries_types.hxx:298-330) is 0, and any
+ * operator with a NULL operand is NULL without being evaluated (no row error
+ * is raised for it). */
 static int eval_node(eval_ctx* c, int32_t idx, int64_t row) {
     if (idx < 0 || idx >= c->n_nodes) return -1;
     if (c->done[idx]) return 0;
     const up_expr_node* nd = &c->nodes[idx];
     orc_dec* out = &c->vals[idx];
+    if (nd->left >= 0 || nd->right >= 0) {
+        if (nd->left >= 0 && eval_node(c, nd->left, row)) return -1;
+        if (nd->right >= 0 && eval_node(c, nd->right, row)) return -1;
+        if ((nd->left >= 0 && c->done[nd->left] == EV_NULL) || (nd->right >= 0 && c->done[nd->right] == EV_NULL)) {
+            dec_zero(out);
+            c->done[idx] = EV_NULL;
+            return 0;
+        }
+    }
     switch (nd->kind) {
         case UP_NODE_COLUMN: {
             const up_col_type* t = &c->col_types[nd->column];
             int vb = col_value_bytes(t);
             const uint8_t* p = c->cols[nd->column] + row * vb;
-            if (t->nullable) p += 1; /* flag byte; NULLs are not modelled here */
+            if (t->nullable) {
+                if (p[0] == 0) {
+                    dec_zero(out);
+                    c->done[idx] = EV_NULL;
+                    return 0;
+                }
+                p += 1;
+            }
             orc_decode(p, orc_compact_bytes(t->precision), t->scale, out);
             break;
         }
@@ -567,8 +589,18 @@ static int eval_node(eval_ctx* c, int32_t idx, int64_t row) {
             return -1;
     }
     if (nd->reverse) out->sign ^= 1u; /* operator-(), AriesDecimal.hxx:291-300 */
-    c->done[idx] = 1;
+    c->done[idx] = EV_VALUE;
     return 0;
+}
+
+/* 1 when a nullable column is reachable from node idx */
+static int reaches_nullable(const up_expr_node* nodes, int32_t n_nodes, const up_col_type* col_types, int32_t idx,
+                            int depth) {
+    if (idx < 0 || idx >= n_nodes || depth > n_nodes) return 0;
+    const up_expr_node* nd = &nodes[idx];
+    if (nd->kind == UP_NODE_COLUMN) return col_types[nd->column].nullable != 0;
+    return reaches_nullable(nodes, n_nodes, col_types, nd->left, depth + 1) ||
+           reaches_nullable(nodes, n_nodes, col_types, nd->right, depth + 1);
 }
 
 int32_t orc_eval_expr(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
@@ -585,6 +617,9 @@ int32_t orc_eval_expr(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
     uint32_t all = 0;
     int rc = 0;
     int cmp = is_compare(nodes[root].kind);
+    /* a nullable result (any nullable column in the tree) is a flag byte, 1
+     * for a value, then the value; a NULL row stores flag 0 and zero bytes */
+    const int nullable = reaches_nullable(nodes, n_nodes, col_types, root, 0);
     for (int64_t row = row_begin; row < row_end; row++) {
         memset(c.done, 0, (size_t)n_nodes);
         c.err = 0;
@@ -593,10 +628,21 @@ int32_t orc_eval_expr(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
             break;
         }
         uint8_t* o = out + row * out_bytes;
+        int vbytes = out_bytes;
+        if (nullable) {
+            o[0] = c.done[root] == EV_NULL ? 0 : 1;
+            o += 1;
+            vbytes -= 1;
+            if (c.done[root] == EV_NULL) {
+                memset(o, 0, (size_t)vbytes);
+                if (row_err) row_err[row] = 0;
+                continue;
+            }
+        }
         if (cmp) {
             o[0] = (uint8_t)(c.vals[root].n != 0);
         } else {
-            c.err |= orc_encode(&c.vals[root], out_bytes, o);
+            c.err |= orc_encode(&c.vals[root], vbytes, o);
         }
         if (row_err) row_err[row] = (uint8_t)c.err;
         all |= c.err;
@@ -688,6 +734,21 @@ static void count_to_dec(int64_t cnt, orc_dec* d) {
     d->n = bn_trim(d->m, 2);
 }
 
+/* nullable_type<Decimal> /= int64 (aries_types.hxx:626-631): the value is
+ * divided by Decimal::DivOrMod (decimal.cu:2200-2228) and the flag survives
+ * only a nonzero divisor.  DivOrMod raises frac by 4 first; a zero dividend
+ * then returns +0 with prec = frac + 1; a zero divisor leaves the value and
+ * sets error = ERR_DIV_BY_ZERO (decimal.hxx:28). */
+static void write_avg_image(uint8_t* img, int sum_flag, int64_t count, const orc_dec* dividend,
+                            const orc_dec* r, uint32_t e) {
+    write_agg_image(img, sum_flag && count != 0, r);
+    if (dividend->n == 0) {
+        img[1] = 0;
+        img[2] = (uint8_t)(r->frac + 1);
+    }
+    if (e & UP_ROWERR_DIV_BY_ZERO) img[4] = 2;
+}
+
 void orc_division_int64(const uint8_t* sum_img, int64_t count, uint8_t* out_img) {
     orc_dec* s = (orc_dec*)malloc(3 * sizeof(orc_dec));
     orc_dec* c = s + 1;
@@ -695,8 +756,7 @@ void orc_division_int64(const uint8_t* sum_img, int64_t count, uint8_t* out_img)
     read_agg_image(sum_img, s);
     count_to_dec(count, c);
     uint32_t e = orc_div(r, s, c);
-    write_agg_image(out_img, sum_img[0], r);
-    if (e & UP_ROWERR_DIV_BY_ZERO) out_img[4] = 2; /* Decimal::error = ERR_DIV_BY_ZERO */
+    write_avg_image(out_img, sum_img[0] != 0, count, s, r, e);
     free(s);
 }
 
@@ -708,16 +768,17 @@ static void finalize_group(uint8_t* out, int32_t kind, orc_dec* sum, int64_t cnt
     }
     if (sum->n == 0) sum->sign = 0; /* -0 from cancellation normalised to +0 */
     uint8_t* img = out + (int64_t)UP_AGG_DECIMAL_BYTES * g;
-    if (kind == UP_AGG_SUM || cnt == 0) {
+    if (kind == UP_AGG_SUM) {
         write_agg_image(img, cnt > 0, sum);
-        if (kind == UP_AGG_AVG) img[3] = (uint8_t)(sum->frac + 4);
         return;
     }
+    /* AVG = DivisionInt64 of the SUM by the count; a group without rows has a
+     * zero sum, which the divide rule's zero-dividend case handles */
     orc_dec* c = (orc_dec*)malloc(2 * sizeof(orc_dec));
     orc_dec* r = c + 1;
     count_to_dec(cnt, c);
-    orc_div(r, sum, c);
-    write_agg_image(img, 1, r);
+    uint32_t e = orc_div(r, sum, c);
+    write_avg_image(img, cnt > 0, cnt, sum, r, e);
     free(c);
 }
 
@@ -756,7 +817,8 @@ typedef struct {
     int64_t b, e;
     int32_t n_groups;
     orc_dec* sums;   /* [n_aggs][n_groups] */
-    int64_t* cnts;   /* [n_groups] */
+    int64_t* cnts;   /* [n_groups]: rows of the group (COUNT(*)) */
+    int64_t* acnts;  /* [n_aggs][n_groups]: rows whose aggregated expression is not NULL */
 } query_job;
 
 static void* query_thread(void* arg) {
@@ -778,6 +840,9 @@ static void* query_thread(void* arg) {
             if (j->aggs[a].kind == UP_AGG_COUNT) continue;
             c.err = 0;
             eval_node(&c, j->aggs[a].root, row);
+            /* SUM/AVG skip NULLs (agg_sum_t on nullable_type, operators.hxx:1176-1193) */
+            if (c.done[j->aggs[a].root] == EV_NULL) continue;
+            j->acnts[(int64_t)a * j->n_groups + g]++;
             orc_dec* s = &j->sums[(int64_t)a * j->n_groups + g];
             orc_add(t, s, &c.vals[j->aggs[a].root]);
             dec_copy(s, t);
@@ -812,6 +877,7 @@ int32_t orc_query(const up_expr_node* nodes, int32_t n_nodes,
         j->n_groups = n_groups;
         j->sums = (orc_dec*)calloc((size_t)n_aggs * (size_t)n_groups, sizeof(orc_dec));
         j->cnts = (int64_t*)calloc((size_t)n_groups, sizeof(int64_t));
+        j->acnts = (int64_t*)calloc((size_t)n_aggs * (size_t)n_groups, sizeof(int64_t));
         for (int32_t a = 0; a < n_aggs; a++)
             for (int32_t g = 0; g < n_groups; g++)
                 j->sums[(int64_t)a * n_groups + g].frac = nodes[aggs[a].root].scale;
@@ -822,6 +888,7 @@ int32_t orc_query(const up_expr_node* nodes, int32_t n_nodes,
     orc_dec* tmp = (orc_dec*)malloc(sizeof(orc_dec));
     for (int t = 1; t < threads; t++) {
         for (int32_t g = 0; g < n_groups; g++) jobs[0].cnts[g] += jobs[t].cnts[g];
+        for (int64_t k = 0; k < (int64_t)n_aggs * n_groups; k++) jobs[0].acnts[k] += jobs[t].acnts[k];
         for (int64_t k = 0; k < (int64_t)n_aggs * n_groups; k++) {
             orc_add(tmp, &jobs[0].sums[k], &jobs[t].sums[k]);
             dec_copy(&jobs[0].sums[k], tmp);
@@ -831,10 +898,12 @@ int32_t orc_query(const up_expr_node* nodes, int32_t n_nodes,
     for (int32_t a = 0; a < n_aggs; a++)
         for (int32_t g = 0; g < n_groups; g++)
             finalize_group(outs[a], aggs[a].kind, &jobs[0].sums[(int64_t)a * n_groups + g],
-                           jobs[0].cnts[g], g);
+                           aggs[a].kind == UP_AGG_COUNT ? jobs[0].cnts[g] : jobs[0].acnts[(int64_t)a * n_groups + g],
+                           g);
     for (int t = 0; t < threads; t++) {
         free(jobs[t].sums);
         free(jobs[t].cnts);
+        free(jobs[t].acnts);
     }
     free(jobs);
     free(th);

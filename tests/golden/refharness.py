@@ -92,3 +92,95 @@ def run(op: str, a_dev, pa, sa, b_dev, pb, sb, rows, out_dev, out_bytes, c_dev=N
     if rc != 0:
         raise RuntimeError(f"reference harness refused or failed: {rc} (op {op}, LEN {L})")
     return L
+
+
+# ------------------------------------------------------------------------
+# The 32-limb Decimal harness (oracle/_ref/libariesref_agg.so): grouped SUM by
+# the XMP segmented-reduction add, AVG by Decimal /= int64, CSV-import text
+# parse and GetDecimal text output, each run by the reference's own code.
+AGG_LIB = os.path.join(ROOT, "oracle", "_ref", "libariesref_agg.so")
+_agg = None
+FORMAT_WIDTH = 8 * 32 + 8
+
+
+def agg_available() -> bool:
+    return os.path.exists(AGG_LIB)
+
+
+def agg_load():
+    global _agg
+    if _agg is None:
+        lib = C.CDLL(AGG_LIB)
+        P = C.c_void_p
+        lib.refagg_compact_bytes.restype = C.c_int
+        lib.refagg_compact_bytes.argtypes = [C.c_int]
+        lib.refagg_sum.restype = C.c_int
+        lib.refagg_sum.argtypes = [P, C.c_int, C.c_int, P, P, C.c_int, C.c_int64, P]
+        lib.refagg_div_int64.restype = C.c_int
+        lib.refagg_div_int64.argtypes = [P, P, C.c_int, P]
+        lib.refagg_parse.restype = C.c_int
+        lib.refagg_parse.argtypes = [P, P, P, C.c_int64, C.c_int, C.c_int, P, P]
+        lib.refagg_format.restype = C.c_int
+        lib.refagg_format.argtypes = [P, C.c_int64, C.c_int, C.c_int, P, C.c_int]
+        _agg = lib
+    return _agg
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"reference harness refused or failed: {rc} ({what})")
+
+
+def sum_segments(vals: bytes, prec: int, scale: int, starts, rows: int, assoc=None) -> bytes:
+    """133-byte SUM images of each segment [starts[g], starts[g+1]) of a host
+    compact column (visited through `assoc` when given)."""
+    import torch
+    lib = agg_load()
+    d = torch.frombuffer(bytearray(vals or b"\0"), dtype=torch.uint8).cuda()
+    st = torch.tensor(list(starts) or [0], dtype=torch.int32).cuda()
+    asc = torch.tensor(list(assoc), dtype=torch.int32).cuda() if assoc is not None else None
+    out = torch.zeros(max(1, len(starts)) * 133, dtype=torch.uint8).cuda()
+    _check(lib.refagg_sum(d.data_ptr(), prec, scale, asc.data_ptr() if asc is not None else None, st.data_ptr(),
+                          len(starts), rows, out.data_ptr()), "sum")
+    return bytes(out.cpu().numpy().tobytes())[:len(starts) * 133]
+
+
+def div_int64(images: bytes, counts) -> bytes:
+    import torch
+    lib = agg_load()
+    n = len(counts)
+    s = torch.frombuffer(bytearray(images or b"\0"), dtype=torch.uint8).cuda()
+    c = torch.tensor(list(counts) or [0], dtype=torch.int64).cuda()
+    out = torch.zeros(max(1, n) * 133, dtype=torch.uint8).cuda()
+    _check(lib.refagg_div_int64(s.data_ptr(), c.data_ptr(), n, out.data_ptr()), "div_int64")
+    return bytes(out.cpu().numpy().tobytes())[:n * 133]
+
+
+def parse(fields, prec: int, scale: int):
+    """(compact bytes, per-row error codes) of text fields."""
+    import torch
+    lib = agg_load()
+    text = b"".join(fields)
+    offs = [0]
+    for f in fields:
+        offs.append(offs[-1] + len(f))
+    host_offs = (C.c_int64 * len(offs))(*offs)
+    t = torch.frombuffer(bytearray(text or b"\0"), dtype=torch.uint8).cuda()
+    o = torch.tensor(offs, dtype=torch.int64).cuda()
+    nb = lib.refagg_compact_bytes(prec)
+    out = torch.zeros(max(1, len(fields) * nb), dtype=torch.uint8).cuda()
+    err = torch.zeros(max(1, len(fields)), dtype=torch.uint8).cuda()
+    _check(lib.refagg_parse(t.data_ptr(), o.data_ptr(), host_offs, len(fields), prec, scale, out.data_ptr(),
+                            err.data_ptr()), "parse")
+    return bytes(out.cpu().numpy().tobytes())[:len(fields) * nb], bytes(err.cpu().numpy().tobytes())[:len(fields)]
+
+
+def format_hex(compact: bytes, rows: int, prec: int, scale: int):
+    """GetDecimal strings of a host compact column."""
+    import torch
+    lib = agg_load()
+    d = torch.frombuffer(bytearray(compact or b"\0"), dtype=torch.uint8).cuda()
+    out = torch.zeros(max(1, rows) * FORMAT_WIDTH, dtype=torch.uint8).cuda()
+    _check(lib.refagg_format(d.data_ptr(), rows, prec, scale, out.data_ptr(), FORMAT_WIDTH), "format")
+    raw = bytes(out.cpu().numpy().tobytes())
+    return [raw[i * FORMAT_WIDTH:(i + 1) * FORMAT_WIDTH].split(b"\0", 1)[0].decode() for i in range(rows)]

@@ -171,3 +171,50 @@ def test_boolean_typing_rejects_mixed_children():
         built = E.build([bad], cols)
         with pytest.raises(A.UpError):
             E.derive_types(built)
+
+
+def test_oracle_null_semantics():
+    """NULL handling of the oracle (the rules the GPU tests check the CUDA path
+    against): a nullable value's flag byte 0 is NULL; an expression over a NULL
+    is NULL (flag 0, zero value bytes, no row error); SUM/AVG skip NULL rows,
+    a group without any non-NULL row has SUM and AVG flag 0, COUNT counts all
+    rows of the group."""
+    import numpy as np
+    from oracle import oracle, pyref
+    from ultraprecise_b200 import abi, codec
+    from ultraprecise_b200 import expr as E
+    nb = codec.compact_bytes(15)
+    vals = [(0, 1234), (1, 50), (0, 7), (0, 0), (1, 999)]
+    flags = [1, 0, 1, 0, 1]
+    rx = b"".join(bytes([f]) + codec.encode([v], 15) for f, v in zip(flags, vals))
+    ry = codec.encode([(0, 3), (0, 4), (0, 5), (0, 6), (0, 7)], 15)
+    ct = [E.ColType(15, 2, nullable=True), E.ColType(15, 2)]
+    x, y = E.col(0), E.col(1)
+    b = E.build([x * y], ct)
+    E.derive_types(b)
+    ob = codec.compact_bytes(b.nodes[b.roots[0]].precision) + 1
+    out, err = oracle.eval_expr(b, b.roots[0], [rx, ry], 5, ob)
+    assert err == 0
+    for i in range(5):
+        row = out[i * ob:(i + 1) * ob]
+        assert row[0] == flags[i]
+        if flags[i]:
+            (s, m, _) = pyref.mul(pyref.decode(codec.encode([vals[i]], 15), 2),
+                                  pyref.decode(ry[i * nb:(i + 1) * nb], 2))
+            assert row[1:] == pyref.encode((s, m, 4), ob - 1)[0]
+        else:
+            assert not any(row[1:])
+    # grouped: groups 0,0,1,1,0 -> group 1 holds rows 2 (value) and 3 (NULL)
+    q = E.build([x, x * y], ct)
+    E.derive_types(q)
+    gid = np.array([0, 0, 1, 1, 2], dtype=np.int32).tobytes()
+    # group 2 gets only row 4 (a value); a group 3 has no rows at all
+    aggs = [(abi.UP_AGG_SUM, q.roots[0]), (abi.UP_AGG_AVG, q.roots[1]), (abi.UP_AGG_COUNT, q.roots[0])]
+    s_img, a_img, cnt = oracle.query(q, aggs, [rx, ry], gid, 5, 4)
+    img = abi.UP_AGG_DECIMAL_BYTES
+    counts = np.frombuffer(cnt, dtype=np.int64).tolist()
+    assert counts == [2, 2, 1, 0]                              # COUNT(*): NULL rows counted
+    assert int.from_bytes(s_img[5:img], "little") == 1234       # group 0: the NULL row is skipped
+    assert s_img[img] == 1 and s_img[3 * img] == 0              # group 1 has a value, group 3 none
+    g1_avg = a_img[img:2 * img]
+    assert g1_avg[0] == 1 and int.from_bytes(g1_avg[5:], "little") == 7 * 5 * 10000  # AVG over 1 non-NULL row
