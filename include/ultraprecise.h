@@ -53,7 +53,8 @@ enum {
 enum {
     UP_ROWERR_OVERFLOW = 1u,     /* the value did not fit the compact field: bits were lost */
     UP_ROWERR_DIV_BY_ZERO = 2u,  /* a divisor was zero (ERR_DIV_BY_ZERO, decimal.hxx:28) */
-    UP_ROWERR_DOMAIN = 4u        /* an input outside the supported domain (e.g. bad group id) */
+    UP_ROWERR_DOMAIN = 4u,       /* an input outside the supported domain (e.g. bad group id) */
+    UP_ROWERR_TIMEOUT = 8u       /* a bounded wait in the kernel ran out: the launch's results are incomplete */
 };
 
 const char* up_status_string(up_status s);
@@ -178,6 +179,20 @@ int64_t up_module_source(const up_module* m, char* buf, int64_t cap);
  * `err_word` (device uint32, may be NULL) receives UP_ROWERR_* bits OR-ed. */
 up_status up_expr_launch(up_module* m, const up_column* in, int32_t n_in, int64_t rows,
                          void* out, uint32_t* err_word, void* stream);
+/* One launch over n_req requests of the same expression module: request k
+ * reads columns in[k*n_in .. k*n_in+n_in) over rows[k] rows and writes outs[k];
+ * errs[k] (device uint32, may be NULL) receives its row errors.  Requests of
+ * contiguous non-null columns on a one-thread-per-value module share one
+ * kernel (virtual tiles over all requests); otherwise each request is launched
+ * on its own.  Results equal launching each request alone.  The request
+ * descriptors go through a stream-ordered allocation.  No counterpart in the
+ * reference (one kernel per expression and call, DynamicKernel.cu:281-338). */
+up_status up_expr_launch_many(up_module* m, const up_column* in, int32_t n_in, const int64_t* rows, int32_t n_req,
+                              void* const* outs, uint32_t* const* errs, void* stream);
+
+/* Threads that cooperate on one value in the module's kernel (1: one thread
+ * per value; 2..32: the cooperative form), as chosen at compile time. */
+int32_t up_module_threads_per_value(const up_module* m);
 void up_module_release(up_module* m);
 /* Number of cached compiled kernels; clears the cache when clear != 0. */
 int32_t up_module_cache_size(int32_t clear);

@@ -9,7 +9,9 @@
  * session's device-memory budget (free memory at creation minus a reserve,
  * optionally capped) covers their outputs and scratch, and launches every
  * admitted request at once across the streams, while earlier ones still run
- * (continuous batching).  Each request's completion time is stamped by a host
+ * (continuous batching); requests of the same expression module admitted in
+ * one dispatch share one merged launch (opts.merge), and an optional window
+ * lets a dispatch wait briefly for more arrivals to merge.  Each request's completion time is stamped by a host
  * callback on its stream; latency = completion - arrival.  Results are
  * byte-identical to launching the same module alone.
  */
@@ -31,6 +33,11 @@ typedef struct up_serve_opts {
     int64_t reserve_bytes;     /* device memory left free (0 = 2 GiB) */
     double heavy_work;         /* > 0: estimated limb work (rows x per-row work) above which a request runs on a
                                   low-priority stream with one CTA per tile; <= 0: off (all streams equal) */
+    int32_t merge;             /* 1: requests of one expression module admitted together run as one merged
+                                  launch (up_expr_launch_many); 0: one launch per request */
+    int32_t max_batch;         /* most requests the scheduler admits per dispatch (0 = 256) */
+    double batch_window_us;    /* > 0: after the first request of a dispatch, wait up to this long for more
+                                  arrivals to admit with it (continuous batching window); 0: dispatch at once */
 } up_serve_opts;
 
 typedef struct up_serve_request {
@@ -75,6 +82,8 @@ typedef struct up_serve_stats {
     int32_t max_inflight_seen;
     int32_t pad;
     double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;   /* over requests completed since the last reset */
+    int64_t merged_launches;       /* merged launches so far, and the requests they ran */
+    int64_t merged_requests;
 } up_serve_stats;
 
 up_status up_serve_stats_get(up_serve* s, int32_t reset, up_serve_stats* out);

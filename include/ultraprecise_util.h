@@ -33,10 +33,19 @@ up_status up_util_gen_range(void* out, int64_t rows, int32_t precision, int64_t 
 /* Write `bytes` of a scratch buffer (DEVICE) to evict L2. */
 up_status up_util_flush_l2(void* buf, int64_t bytes, void* stream);
 
-/* Measure the 32-bit integer multiply-add throughput of the current device:
- * a dependent-free chain of 64-bit-accumulating multiply-adds (the operation
- * the limb multiply loops issue).  Returns multiply-adds per second. */
+/* Measure the limb multiply-add throughput of the current device: 32 x 32
+ * -> 64-bit products added to 64-bit accumulators (the operation the limb
+ * multiply loops issue), eight independent chains per thread, nothing else
+ * in the loop.  Returns multiply-adds per second. */
 up_status up_util_imad_peak(double* madds_per_s, void* stream);
+
+/* Make the bounded wait of the bulk-copy pipelines run out, on purpose and
+ * safely: one block waits with `polls` polls (1 .. 2^24) on an mbarrier armed
+ * for bytes that no copy ever delivers, then reports UP_ROWERR_TIMEOUT in
+ * *err_word (DEVICE) the way the tile kernels do, and adds 1 to *done_word
+ * (DEVICE) when it has returned.  Nothing is left in flight; the context stays
+ * usable.  For testing the timeout path. */
+up_status up_util_wait_timeout_probe(uint32_t polls, uint32_t* err_word, uint32_t* done_word, void* stream);
 
 /* Compile a kernel source with the library's NVRTC settings without loading
  * it (no GPU needed).  Returns UP_OK or UP_ERR_COMPILE with the log in

@@ -31,7 +31,7 @@ def _rank_main(rank, world, port, out):
     try:
         bench.barrier(world)
         mx = bench.max_over_ranks(10.0 * (rank + 1), world)
-        args = types.SimpleNamespace(workload="sweep", steps=1, warmup=0, cpu_seconds=0.2)
+        args = types.SimpleNamespace(workload="sweep", steps=1, warmup=0, cpu_seconds=0.2, ref_seconds=0.5)
         ref = bench.run_reference(args, rank, world)
         bench.barrier(world)
         out[rank] = (mx, ref is None, None if ref is None else (ref["impl"], ref["n_gpus"], ref["unit"]))

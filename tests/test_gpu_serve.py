@@ -99,3 +99,54 @@ def test_request_larger_than_budget_is_refused(shapes):
         sess.submit(s["mod"], s["cols"], s["rows"])
     assert ei.value.status == abi.UP_ERR_NO_MEMORY
     sess.close()
+
+
+def test_merged_launch_matches_requests_alone(shapes):
+    """up_expr_launch_many: several requests of one module in one kernel
+    (different row counts, an empty request, offset column bases) give the
+    bytes and row errors of each request launched alone."""
+    import ctypes as C
+    s = shapes[1]  # p=76 division: row errors occur (quotients that overflow the result type)
+    lib = abi.load()
+    vb = s["cols"][0].value_bytes
+    reqs = [(0, s["rows"]), (17, 1000), (5, 0), (123, 20_000), (1, 333)]  # (first row, rows)
+    ins, rows, outs, errs, alone = [], [], [], [], []
+    for r0, n in reqs:
+        cols = [runtime.DeviceColumn(c.data[r0 * vb:], c.precision, c.scale) for c in s["cols"]]
+        ins += [c.up_column() for c in cols]
+        rows.append(n)
+        outs.append(torch.full((max(1, n * s["mod"].value_bytes),), 0x3C, dtype=torch.uint8, device="cuda"))
+        errs.append(torch.zeros(1, dtype=torch.int32, device="cuda"))
+        e1 = torch.zeros(1, dtype=torch.int32, device="cuda")
+        alone.append((bytes(s["mod"].launch(cols, n, err=e1).cpu().numpy().tobytes()) if n else b"", e1))
+    arr = (abi.UpColumn * len(ins))(*ins)
+    rr = (C.c_int64 * len(rows))(*rows)
+    oo = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+    ee = (C.c_void_p * len(errs))(*[e.data_ptr() for e in errs])
+    abi.check(lib.up_expr_launch_many(s["mod"]._h, arr, len(s["cols"]), rr, len(reqs), oo, ee,
+                                      torch.cuda.current_stream().cuda_stream), "up_expr_launch_many")
+    torch.cuda.synchronize()
+    for (r0, n), o, e, (a, ae) in zip(reqs, outs, errs, alone):
+        assert bytes(o[:n * s["mod"].value_bytes].cpu().numpy().tobytes()) == a
+        assert int(e.item()) == int(ae.item())
+
+
+def test_session_merges_same_module_requests(shapes):
+    """With merging on and a batching window, requests of one expression
+    module admitted together run as merged launches; every result still
+    equals the request run alone."""
+    sess = serve.Session(n_streams=4, merge=True, batch_window_us=2000.0)
+    ids = []
+    for i in range(60):
+        s = shapes[i % 3]  # expression shapes only
+        ids.append((sess.submit(s["mod"], s["cols"], s["rows"]), s))
+    for rid, s in ids:
+        assert sess.wait(rid, 60_000) == serve.DONE
+        out, err = sess.result(rid, 0)
+        assert err == s["err"]
+        assert bytes(out.cpu().numpy().tobytes()) == s["alone"][0]
+        sess.release(rid)
+    st = sess.stats()
+    assert st["completed"] == 60 and st["failed"] == 0
+    assert st["merged_launches"] >= 1 and st["merged_requests"] >= 2
+    sess.close()

@@ -23,6 +23,7 @@ UP_ERR_NO_DEVICE = 9
 UP_ROWERR_OVERFLOW = 1
 UP_ROWERR_DIV_BY_ZERO = 2
 UP_ROWERR_DOMAIN = 4
+UP_ROWERR_TIMEOUT = 8
 
 UP_NODE_COLUMN = 0
 UP_NODE_CONST = 1
@@ -136,6 +137,8 @@ SIGNATURES = {
     "up_format_width": (_I32, [_I32, _I32]),
     "up_format_decimal": (_I32, [_P, _I64, _I32, _I32, _I32, _P, _I32, _P, _P]),
     "up_expr_launch_host": (_I32, [_P, _P, _I32, _I64, _P, C.POINTER(C.c_uint32), _I64]),
+    "up_module_threads_per_value": (_I32, [_P]),
+    "up_expr_launch_many": (_I32, [_P, _P, _I32, _P, _I32, _P, _P, _P]),
     "up_module_release": (None, [_P]),
     "up_module_cache_size": (_I32, [_I32]),
     "up_group_agg": (_I32, [_P, _P, _I32, _P, _I32, _I64, _P, _P, _P]),

@@ -1,5 +1,6 @@
-"""Prototypes of the entry points declared in include/ultraprecise_util.h
-and include/ultraprecise_batch.h / ultraprecise_serve.h."""
+"""Prototypes of the entry points declared in include/ultraprecise_util.h,
+include/ultraprecise_batch.h, ultraprecise_serve.h and
+ultraprecise_costmodel.h."""
 import ctypes as C
 
 _P = C.c_void_p
@@ -12,6 +13,7 @@ SIGNATURES = {
     "up_util_gen_range": (_I32, [_P, _I64, _I32, _I64, _I64, _I64, _U64, _P]),
     "up_util_flush_l2": (_I32, [_P, _I64, _P]),
     "up_util_imad_peak": (_I32, [C.POINTER(C.c_double), _P]),
+    "up_util_wait_timeout_probe": (_I32, [C.c_uint32, _P, _P, _P]),
     "up_util_compile_only": (_I32, [_P, _I32, _I32, _P, _I32, _I32, _P, _I32]),
     "up_util_compile_expr_only": (_I32, [_P, _I32, _I32, _P, _I32, _P]),
     "up_util_expr_source": (_I64, [_P, _I32, _I32, _P, _I32, _P, C.c_char_p, _I64]),
@@ -33,4 +35,15 @@ SIGNATURES = {
     "up_serve_release": (_I32, [_P, _I64]),
     "up_serve_stats_get": (_I32, [_P, _I32, _P]),
     "up_serve_destroy": (None, [_P]),
+    # ultraprecise_costmodel.h
+    "up_costmodel_create": (_I32, [_U64, C.POINTER(_P)]),
+    "up_costmodel_release": (None, [_P]),
+    "up_costmodel_expr_features": (_I32, [_P, _I32, _I32, _P, _I32, _I32, _I64, _P, C.POINTER(_I32)]),
+    "up_costmodel_train": (_I32, [_P, _P, _P, _I32, _I32, _I32, C.c_float, _U64, C.POINTER(C.c_float)]),
+    "up_costmodel_predict": (_I32, [_P, _P, _I32, _P]),
+    "up_costmodel_gradients": (_I32, [_P, _P, _P, _I32, _P, C.POINTER(C.c_float)]),
+    "up_costmodel_get_params": (_I32, [_P, _P, _P]),
+    "up_costmodel_set_params": (_I32, [_P, _P, _P]),
+    "up_costmodel_choose_tpv": (_I32, [_P, _P, _I32, _I32, _P, _I32, _I64, C.POINTER(_I32), C.POINTER(C.c_float)]),
+    "up_costmodel_set_default": (_I32, [_P]),
 }

@@ -28,8 +28,8 @@ GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CXX_SOURCES = ["up_host.cpp", "up_typing.cpp", "up_align.cpp", "up_codegen.cpp", "up_jit.cpp", "up_abi.cpp",
                "up_batch.cpp", "up_serve.cpp"]
-CU_SOURCES = ["up_kernels.cu", "up_noalloc.cu", "up_text.cu", "up_filter.cu"]
-HEADERS = ["up_internal.h", "up_kernels.h", "up_dev.cuh", "up_batch.h"]
+CU_SOURCES = ["up_kernels.cu", "up_noalloc.cu", "up_text.cu", "up_filter.cu", "up_costmodel.cu"]
+HEADERS = ["up_internal.h", "up_kernels.h", "up_dev.cuh", "up_batch.h", "up_kargs.h"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:
@@ -40,13 +40,15 @@ def _newer(target: str, deps: list[str]) -> bool:
 
 
 def _embed_header() -> str:
-    src = os.path.join(CSRC, "up_dev.cuh")
+    """The device headers the JIT hands to NVRTC, as C string literals."""
+    srcs = [("kUpDevCuh", os.path.join(CSRC, "up_dev.cuh")), ("kUpKargsH", os.path.join(CSRC, "up_kargs.h"))]
     dst = os.path.join(OBJ, "up_dev_embed.inc")
-    if _newer(dst, [src]):
-        text = open(src).read()
-        assert ')UPDEV"' not in text
+    if _newer(dst, [p for _, p in srcs]):
         with open(dst + ".tmp", "w") as f:
-            f.write('static const char kUpDevCuh[] = R"UPDEV(' + text + ')UPDEV";\n')
+            for name, path in srcs:
+                text = open(path).read()
+                assert ')UPDEV"' not in text
+                f.write(f'static const char {name}[] = R"UPDEV(' + text + ')UPDEV";\n')
         os.replace(dst + ".tmp", dst)
     return dst
 
@@ -89,7 +91,7 @@ def build(jobs: int = 8, clean: bool = False, verbose: bool = False) -> str:
     if cmds or not os.path.exists(OUT):
         tmp = OUT + ".tmp"
         _run(["g++", "-shared", "-o", tmp, *objs, f"-L{CUDA}/lib64", "-lcudart_static", "-lnvrtc",
-              "-ldl", "-lrt", "-lpthread", f"-Wl,-rpath,{CUDA}/lib64"])
+              "-lz", "-ldl", "-lrt", "-lpthread", f"-Wl,-rpath,{CUDA}/lib64"])
         os.replace(tmp, OUT)
     if verbose:
         print(f"built {OUT} ({len(cmds)} compiled)")

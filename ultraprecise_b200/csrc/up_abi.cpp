@@ -14,44 +14,13 @@ using namespace upi;
 
 namespace {
 
-// Host mirror of the device-side argument blocks emitted by the code
-// generator (KCol in up_dev.cuh; UpArgs / UpQArgs in up_codegen.cpp).
-struct HKCol {
-    const void* data;
-    const void* const* blocks;
-    const int64_t* prefix;
-    const int32_t* indices;
-    int32_t n_blocks;
-    int32_t value_bytes;
-};
-static_assert(sizeof(HKCol) == 40, "KCol layout");
-constexpr int kMaxCols = 16;
-constexpr int kMaxAggs = 16;
-struct HUpArgs {
-    HKCol col[kMaxCols];
-    int64_t rows;
-    uint8_t* out;
-    uint32_t* err;
-    int32_t vec_ok;
-    int32_t out_nullable;
-};
-static_assert(sizeof(HUpArgs) == 672, "UpArgs layout");
-struct HUpQArgs {
-    HKCol col[kMaxCols];
-    uint8_t* out[kMaxAggs];
-    int64_t rows;
-    const int32_t* gid;
-    uint32_t* acc;
-    uint64_t* cnt;
-    uint32_t* err;
-    int32_t n_groups;
-    int32_t vec_ok;
-    const uint8_t* key0;
-    const uint8_t* key1;
-    const int32_t* key_table;
-    int32_t key_mode;
-};
-static_assert(sizeof(HUpQArgs) == 848, "UpQArgs layout");
+// The kernels' argument blocks (UpKCol, UpArgs, UpQArgs) come from
+// up_kargs.h, the header the generated kernels include as well.
+constexpr int kMaxCols = UP_MAX_COLS;
+constexpr int kMaxAggs = UP_MAX_AGGS;
+using HKCol = UpKCol;
+using HUpArgs = UpArgs;
+using HUpQArgs = UpQArgs;
 
 up_status cuda_fail(cudaError_t e, const char* what) {
     cudaGetLastError();
@@ -89,9 +58,9 @@ up_status check_columns(const up_module* m, const up_column* in, int n_in, HKCol
         if (!col.data && col.n_blocks <= 0) return fail(UP_ERR_INVALID_ARG, "column has neither data nor blocks");
         if (col.n_blocks > 0 && (!col.blocks || !col.block_prefix))
             return fail(UP_ERR_INVALID_ARG, "block column without block arrays");
-        kc[c].data = col.data;
-        kc[c].blocks = col.blocks;
-        kc[c].prefix = col.block_prefix;
+        kc[c].data = (const unsigned char*)col.data;
+        kc[c].blocks = (const unsigned char* const*)col.blocks;
+        kc[c].prefix = (const long long*)col.block_prefix;
         kc[c].indices = col.indices;
         kc[c].n_blocks = col.n_blocks > 0 ? col.n_blocks : 0;
         kc[c].value_bytes = col.value_bytes;
@@ -173,6 +142,72 @@ up_status up_module_compile(const up_expr_node* nodes, int32_t n_nodes, int32_t 
     m->jm.gen = std::move(gen);
     m->is_query = false;
     *out = m;
+    return UP_OK;
+}
+
+int32_t up_module_threads_per_value(const up_module* m) { return m ? m->jm.gen.threads_per_value : 0; }
+
+up_status up_expr_launch_many(up_module* m, const up_column* in, int32_t n_in, const int64_t* rows, int32_t n_req,
+                              void* const* outs, uint32_t* const* errs, void* stream) {
+    if (!m || m->is_query) return fail(UP_ERR_INVALID_ARG, "not an expression module");
+    if (n_req < 0 || (n_req > 0 && (!rows || !outs || (n_in > 0 && !in))))
+        return fail(UP_ERR_INVALID_ARG, "bad request arrays");
+    const GeneratedModule& g = m->jm.gen;
+    std::vector<UpMultiReq> reqs;
+    std::vector<int> alone;
+    long long tiles = 0;
+    for (int k = 0; k < n_req; k++) {
+        if (rows[k] < 0) return fail(UP_ERR_INVALID_ARG, "negative row count");
+        if (rows[k] == 0) continue;
+        if (!outs[k]) return fail(UP_ERR_INVALID_ARG, "output is NULL");
+        UpMultiReq q;
+        memset(&q, 0, sizeof q);
+        bool contig = true, vec_ok = true;
+        up_status st = check_columns(m, in + (size_t)k * n_in, n_in, q.col, contig, vec_ok);
+        if (st != UP_OK) return st;
+        if (g.multi_rows == 0 || !contig) {
+            alone.push_back(k);
+            continue;
+        }
+        q.rows = rows[k];
+        q.out = (unsigned char*)outs[k];
+        q.err = errs ? errs[k] : nullptr;
+        q.tile0 = tiles;
+        q.vec_ok = (vec_ok && aligned16(outs[k])) ? 1 : 0;
+        tiles += (rows[k] + g.multi_rows - 1) / g.multi_rows;
+        reqs.push_back(q);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int k : alone) {
+        up_status st = expr_launch_ex(m, in + (size_t)k * n_in, n_in, rows[k], outs[k], errs ? errs[k] : nullptr,
+                                      stream, false);
+        if (st != UP_OK) return st;
+    }
+    if (reqs.empty()) return UP_OK;
+    const int sms = sm_count_current();
+    if (sms <= 0) return fail(UP_ERR_NO_DEVICE, "no CUDA device");
+    void* k = jit_kernel(*m->jm.ks, "up_expr_multi");
+    if (!k) return fail(UP_ERR_CUDA, "module has no up_expr_multi kernel");
+    up_status st = set_smem(k, g.multi_smem);
+    if (st != UP_OK) return st;
+    UpMultiReq* d = nullptr;
+    const size_t bytes = reqs.size() * sizeof(UpMultiReq);
+    UP_CUDA(cudaMallocAsync((void**)&d, bytes, s));
+    cudaError_t e = cudaMemcpyAsync(d, reqs.data(), bytes, cudaMemcpyHostToDevice, s);
+    UpMultiArgs a;
+    memset(&a, 0, sizeof a);
+    a.req = d;
+    a.n_tiles = tiles;
+    a.n_req = (int)reqs.size();
+    void* args[1] = {&a};
+    if (e == cudaSuccess) {
+        const int64_t cap = (int64_t)sms * occupancy(k, g.multi_threads, g.multi_smem);
+        e = cudaLaunchKernel((const void*)k, dim3((unsigned)std::min<int64_t>(tiles, cap)), dim3(g.multi_threads),
+                             args, (size_t)g.multi_smem, s);
+    }
+    cudaError_t e2 = cudaFreeAsync(d, s);
+    if (e != cudaSuccess) return cuda_fail(e, "up_expr_multi");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaFreeAsync");
     return UP_OK;
 }
 
@@ -358,9 +393,16 @@ up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64
 
 }  // extern "C"
 
+size_t query_scratch_bytes(const GeneratedModule& g, int32_t n_groups) {
+    const size_t accw = (size_t)std::max(g.acc_words_per_group, 1);
+    // the int64 counts follow the accumulators: keep them 16-byte aligned
+    const size_t acc_bytes = (((size_t)n_groups * accw * 4u) + 15u) & ~(size_t)15u;
+    return acc_bytes + (size_t)n_groups * 8u;
+}
+
 up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
                           int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread,
-                          const QueryKeys* keys) {
+                          const QueryKeys* keys, void* caller_scratch, size_t caller_scratch_bytes) {
     if (!m || !m->is_query) return fail(UP_ERR_INVALID_ARG, "not a query module");
     const bool device_count = keys && keys->capacity > 0;
     if (device_count) n_groups = keys->capacity;  // accumulators and outputs sized for the capacity
@@ -382,16 +424,22 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
     if (sms <= 0) return fail(UP_ERR_NO_DEVICE, "no CUDA device");
     cudaStream_t s = (cudaStream_t)stream;
     const size_t accw = (size_t)std::max(g.acc_words_per_group, 1);
-    // the int64 counts follow the accumulators: keep them 16-byte aligned
     const size_t acc_bytes = (((size_t)n_groups * accw * 4u) + 15u) & ~(size_t)15u;
-    const size_t cnt_bytes = (size_t)n_groups * 8u;
-    void* scratch = nullptr;
-    UP_CUDA(cudaMallocAsync(&scratch, acc_bytes + cnt_bytes, s));
-    cudaError_t e = cudaMemsetAsync(scratch, 0, acc_bytes + cnt_bytes, s);
+    const size_t need = query_scratch_bytes(g, n_groups);
+    void* scratch = caller_scratch;
+    if (caller_scratch) {
+        if (need > caller_scratch_bytes)
+            return fail(UP_ERR_INVALID_ARG, "scratch too small: " + std::to_string(n_groups) + " groups need " +
+                                                std::to_string(need) + " bytes, " +
+                                                std::to_string(caller_scratch_bytes) + " given");
+    } else {
+        UP_CUDA(cudaMallocAsync(&scratch, need, s));
+    }
+    cudaError_t e = cudaMemsetAsync(scratch, 0, need, s);
     a.rows = rows;
     a.gid = group_ids;
     a.acc = (uint32_t*)scratch;
-    a.cnt = (uint64_t*)((uint8_t*)scratch + acc_bytes);
+    a.cnt = (unsigned long long*)((uint8_t*)scratch + acc_bytes);
     a.err = err_word;
     a.n_groups = device_count ? -n_groups : n_groups;
     a.vec_ok = vec_ok ? 1 : 0;
@@ -443,7 +491,7 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
         void* k = jit_kernel(*m->jm.ks, "up_query_fin");
         e = cudaLaunchKernel((const void*)k, dim3((unsigned)((n_groups + 255) / 256)), dim3(256), args, 0, s);
     }
-    cudaError_t e2 = cudaFreeAsync(scratch, s);
+    cudaError_t e2 = caller_scratch ? cudaSuccess : cudaFreeAsync(scratch, s);
     if (e != cudaSuccess) return cuda_fail(e, "query launch");
     if (e2 != cudaSuccess) return cuda_fail(e2, "cudaFreeAsync");
     return UP_OK;

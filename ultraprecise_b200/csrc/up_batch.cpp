@@ -18,37 +18,9 @@ using namespace upi;
 
 namespace {
 
-struct HKCol {
-    const void* data;
-    const void* const* blocks;
-    const int64_t* prefix;
-    const int32_t* indices;
-    int32_t n_blocks;
-    int32_t value_bytes;
-};
-// host mirror of the generated BTask / BArgs (generate_batch_module)
-struct HBTask {
-    HKCol col[8];
-    int64_t rows;
-    uint8_t* out;
-    const int32_t* gid;
-    uint32_t* acc;
-    uint64_t* cnt;
-    int32_t n_groups;
-    int32_t words;
-};
-static_assert(sizeof(HBTask) == 368, "BTask layout");
-struct HBArgs {
-    void* tasks;
-    const int32_t* item_task;
-    const int64_t* item_tile;
-    int64_t n_items;
-    unsigned long long* head;
-    uint32_t* err;
-    int32_t tile_rows;
-    int32_t pad;
-};
-static_assert(sizeof(HBArgs) == 56, "BArgs layout");
+// the generated kernels' task and argument blocks (up_kargs.h)
+using HBTask = BTask;
+using HBArgs = BArgs;
 
 const int kThreads[3] = {64, 128, 256};
 constexpr int kSoloStreams = 1;
@@ -203,9 +175,9 @@ up_status build_items(up_batch* b, int band, int tile_rows) {
 HBArgs band_args(up_batch* b, int band, uint32_t* err) {
     HBArgs a;
     memset(&a, 0, sizeof a);
-    a.tasks = b->d_tasks;
+    a.tasks = (BTask*)b->d_tasks;
     a.item_task = b->item_task[band];
-    a.item_tile = b->item_tile[band];
+    a.item_tile = (const long long*)b->item_tile[band];
     a.n_items = b->n_items[band];
     a.head = b->heads + band;
     a.err = err;
@@ -329,7 +301,7 @@ up_status prepare(up_batch* b) {
         }
         if (b->gen.tasks[k].agg < 0) continue;
         dev_tasks[k].acc = (uint32_t*)((uint8_t*)b->scratch + acc_off[k]);
-        dev_tasks[k].cnt = (uint64_t*)((uint8_t*)b->scratch + cnt_off[k]);
+        dev_tasks[k].cnt = (unsigned long long*)((uint8_t*)b->scratch + cnt_off[k]);
     }
     UPB_CUDA(cudaMalloc(&b->d_tasks, nt * sizeof(HBTask)));
     UPB_CUDA(cudaMemcpy(b->d_tasks, dev_tasks.data(), nt * sizeof(HBTask), cudaMemcpyHostToDevice));
@@ -518,7 +490,7 @@ up_status up_batch_bind(up_batch* b, int32_t task, const up_column* in, int32_t 
         if (in[c].value_bytes != gt.in_bytes[c] || !in[c].data || in[c].n_blocks > 0 || in[c].indices ||
             in[c].nullable)
             return fail(UP_ERR_INVALID_ARG, "batch tasks take contiguous non-null columns of the compiled width");
-        h.col[c].data = in[c].data;
+        h.col[c].data = (const unsigned char*)in[c].data;
         h.col[c].value_bytes = in[c].value_bytes;
         if (((uintptr_t)in[c].data & 3u) != 0) words = false;
     }

@@ -7,6 +7,7 @@
 // straight-line limb code with every node's limb count and scale fixed at
 // compile time instead of instantiating one AriesDecimal<LEN> for all nodes.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <map>
 #include <set>
@@ -201,63 +202,13 @@ struct Emitter {
     }
 };
 
-std::string kargs_source() {
-    return R"(
-#define UP_MAX_COLS 16
-#define UP_MAX_AGGS 16
-struct UpArgs {
-    KCol col[UP_MAX_COLS];
-    i64 rows;
-    u8* out;
-    u32* err;
-    int vec_ok;
-    int out_nullable;
-};
-struct UpQArgs {
-    KCol col[UP_MAX_COLS];
-    u8* out[UP_MAX_AGGS];
-    i64 rows;
-    const int* gid;
-    u32* acc;
-    u64* cnt;
-    u32* err;
-    int n_groups;
-    int vec_ok;
-};
-)";
-}
+// The argument blocks themselves (UpArgs, UpQArgs, BTask, BArgs) are declared
+// once, in up_kargs.h, which up_dev.cuh includes for the generated code.
+std::string kargs_source() { return "\n"; }
 
 // Query modules: UpQArgs with the group-key fields and the group lookup.
 std::string query_kargs_source() {
     return R"(
-#define UP_MAX_COLS 16
-#define UP_MAX_AGGS 16
-struct UpArgs {
-    KCol col[UP_MAX_COLS];
-    i64 rows;
-    u8* out;
-    u32* err;
-    int vec_ok;
-    int out_nullable;
-};
-struct UpQArgs {
-    KCol col[UP_MAX_COLS];
-    u8* out[UP_MAX_AGGS];
-    i64 rows;
-    const int* gid;
-    u32* acc;
-    u64* cnt;
-    u32* err;
-    int n_groups;
-    int vec_ok;
-    // key_mode 0: group ids from gid[]; otherwise the group is
-    // key_table[key] with key = key0[r] (1), key0[r] << 8 | key1[r] (2), or
-    // key0[2r] << 8 | key0[2r+1] (3)
-    const u8* key0;
-    const u8* key1;
-    const int* key_table;
-    int key_mode;
-};
 UP_DI int q_group(const UpQArgs& a, i64 row) {
     if (a.key_mode == 0) return a.gid[row];
     u32 key;
@@ -513,6 +464,88 @@ int cooperative_width(const up_expr_node* nodes, const std::vector<NodeFacts>& f
 
 }  // namespace
 
+// ------------------------------------------------- cost-model features
+// Features of launching an expression (ultraprecise_costmodel.h): what the
+// generated kernel's run time depends on — rows, threads per value, limb
+// widths, the multiply and divide work per row, bytes moved per row.
+up_status expr_cost_features(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols, int n_cols,
+                             int tpv, int64_t rows, float* out, bool* coop_ok) {
+    std::vector<NodeFacts> f;
+    std::vector<int> topo;
+    up_status st = analyze_nodes(nodes, n_nodes, cols, n_cols, f, topo, {root});
+    if (st != UP_OK) return st;
+    bool any_nullable = false;
+    std::vector<int> used;
+    int max_limbs = 1, n_mul = 0, n_div = 0, n_add = 0, div_limbs = 0;
+    double mul_work = 0, div_work = 0;
+    for (int k : topo) {
+        const up_expr_node& nd = nodes[k];
+        max_limbs = std::max(max_limbs, f[k].limbs);
+        switch (nd.kind) {
+            case UP_NODE_COLUMN:
+                if (std::find(used.begin(), used.end(), nd.column) == used.end()) used.push_back(nd.column);
+                any_nullable |= cols[nd.column].nullable != 0;
+                break;
+            case UP_NODE_MUL:
+                n_mul++;
+                mul_work += (double)f[nd.left].limbs * f[nd.right].limbs;
+                break;
+            case UP_NODE_DIV:
+            case UP_NODE_MOD: {
+                n_div++;
+                const int lb = f[nd.right].limbs;
+                div_limbs = std::max(div_limbs, lb);
+                const int lx = nd.kind == UP_NODE_DIV
+                                   ? f[nd.left].limbs + limbs_for_bits(big_bitlen(big_pow10(f[nd.right].scale + 4)))
+                                   : f[nd.left].limbs;
+                div_work += (double)(lx - f[nd.left].limbs) * f[nd.left].limbs + (double)std::max(1, lx - lb + 1) * lb;
+                break;
+            }
+            case UP_NODE_RESCALE:
+                if (nd.scale < f[nd.left].scale) {
+                    n_div++;
+                    const int lp = limbs_for_bits(big_bitlen(big_pow10(f[nd.left].scale - nd.scale)));
+                    div_limbs = std::max(div_limbs, lp);
+                    div_work += (double)std::max(1, f[nd.left].limbs - lp + 1) * lp;
+                }
+                break;
+            case UP_NODE_ADD:
+            case UP_NODE_SUB:
+                n_add++;
+                break;
+            default:
+                break;
+        }
+    }
+    const bool cmp_root = is_compare_kind(nodes[root].kind);
+    const int out_bytes = cmp_root ? 1 : compact_bytes(nodes[root].precision);
+    int in_bytes = 0;
+    for (int c : used) in_bytes += compact_bytes(cols[c].precision);
+    const int w = cooperative_width(nodes, f, topo);
+    if (coop_ok) *coop_ok = w > 0 && !any_nullable;
+    const double T = std::max(1, tpv);
+    const double work = mul_work + div_work + (double)n_add * max_limbs;
+    auto lg = [](double x) { return (float)std::log2(std::max(x, 1.0)); };
+    float* o = out;
+    o[0] = lg((double)std::max<int64_t>(rows, 1));
+    o[1] = lg(T);
+    o[2] = lg(max_limbs);
+    o[3] = lg(limbs_for_bits(std::max(1, 8 * out_bytes)));
+    o[4] = lg(1.0 + mul_work);
+    o[5] = lg(1.0 + div_work);
+    o[6] = (float)n_mul;
+    o[7] = (float)n_div;
+    o[8] = (float)n_add;
+    o[9] = lg(std::max(1, in_bytes));
+    o[10] = lg(out_bytes);
+    o[11] = n_div > 0 ? 1.f : 0.f;
+    o[12] = lg(std::max(1, div_limbs));
+    o[13] = lg(1.0 + work / T);
+    o[14] = o[0] + lg(1.0 + work);
+    o[15] = lg(tpv > 1 && w > 0 ? std::ceil((double)w / T) : (double)max_limbs);
+    return UP_OK;
+}
+
 // --------------------------------------------------- expression modules
 up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
                                int n_cols, const up_compile_opts* opts, GeneratedModule& out) {
@@ -590,7 +623,17 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
         for (int k : topo)
             has_div |= nodes[k].kind == UP_NODE_DIV || nodes[k].kind == UP_NODE_MOD ||
                        (nodes[k].kind == UP_NODE_RESCALE && nodes[k].scale < f[nodes[k].left].scale);
-        if (w > 0 && req != 1 && !any_nullable && (req > 1 || (w >= kCoopMinLimbs && !has_div))) {
+        // automatic with a learned cost model set: the threads per value of
+        // the lowest predicted time (ultraprecise_costmodel.h)
+        const CostChoice cc = (req == 0 && w > 0 && !any_nullable)
+                                  ? default_model_choose_tpv(nodes, n_nodes, root, cols, n_cols)
+                                  : CostChoice();
+        if (cc.valid) {
+            if (cc.tpv > 1) {
+                tpiT = cc.tpv;
+                tpiK = (w + tpiT - 1) / tpiT;
+            }
+        } else if (w > 0 && req != 1 && !any_nullable && (req > 1 || (w >= kCoopMinLimbs && !has_div))) {
             if (req > 1) {
                 tpiT = req;
             } else {
@@ -783,6 +826,53 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
     src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
 
+    // Merged launches (the serving loop): one kernel over several requests of
+    // this module; virtual tiles of RM rows map to their request by a binary
+    // search over the requests' first tiles; each tile is staged synchronously.
+    out.multi_rows = 0;
+    if (tpiT == 0 && !any_nullable && !em.out_of_line) {
+        int RM = 1024;
+        while (RM > 32 && (long)RM * row_bytes > 24 * 1024) RM /= 2;
+        std::vector<int> moff;
+        int msm = 0;
+        for (int c : used) {
+            moff.push_back(msm);
+            msm += ((RM * compact_bytes(cols[c].precision) + 16 + 15) / 16) * 16;
+        }
+        const int moff_out = msm;
+        msm += ((RM * BO + 16 + 15) / 16) * 16;
+        const int TM = std::min(256, RM);
+        src << "extern \"C\" __global__ void __launch_bounds__(" << TM << ") up_expr_multi(const UpMultiArgs a) {\n";
+        src << "    extern __shared__ __align__(16) u8 sm[];\n";
+        src << "    constexpr int R = " << RM << ";\n";
+        src << "    for (i64 t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {\n";
+        src << "        int lo = 0, hi = a.n_req - 1;\n";
+        src << "        while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (a.req[mid].tile0 <= t) lo = mid; else hi = mid - 1; }\n";
+        src << "        const UpMultiReq& q = a.req[lo];\n";
+        src << "        const i64 row0 = (t - q.tile0) * (i64)R;\n";
+        src << "        const int nr = (q.rows - row0) < R ? (int)(q.rows - row0) : R;\n";
+        for (size_t i = 0; i < used.size(); i++) {
+            const int c = used[i];
+            const int B = compact_bytes(cols[c].precision);
+            src << "        tile_copy_in(sm + " << moff[i] << ", q.col[" << c << "].data + row0 * " << B << ", nr * " << B
+                << ", q.vec_ok != 0);\n";
+        }
+        src << "        __syncthreads();\n        u32 err = 0u;\n";
+        src << "        for (int r = threadIdx.x; r < nr; r += blockDim.x)\n            err |= up_row(";
+        for (size_t i = 0; i < used.size(); i++)
+            src << "sm + " << moff[i] << " + r * " << compact_bytes(cols[used[i]].precision) << ", ";
+        src << "sm + " << moff_out << " + r * " << BO << ", true);\n";
+        src << "        __syncthreads();\n";
+        src << "        tile_copy_out(q.out + row0 * " << BO << ", sm + " << moff_out << ", nr * " << BO
+            << ", q.vec_ok != 0);\n";
+        src << "        err = __reduce_or_sync(0xffffffffu, err);\n";
+        src << "        if ((threadIdx.x & 31) == 0 && err != 0u && q.err) atomicOr(q.err, err);\n";
+        src << "        __syncthreads();\n    }\n}\n\n";
+        out.multi_rows = RM;
+        out.multi_threads = TM;
+        out.multi_smem = msm;
+    }
+
     // generic kernel: blocks, indirection, nullable values
     const int OB = BO + (any_nullable ? 1 : 0);
     src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_generic(const UpArgs a) {\n";
@@ -813,6 +903,7 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
 
     out.source = src.str();
     out.kernels = {"up_expr_tile", "up_expr_generic"};
+    if (out.multi_rows > 0) out.kernels.push_back("up_expr_multi");
     out.work_per_row = em.work + row_bytes;
     out.out_precision = out_p;
     out.out_scale = out_s;
@@ -870,6 +961,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     // one accumulator per distinct aggregated expression (SUM(x) and AVG(x)
     // share one), sized for a sign bit and 2^40 rows above the value bound
     std::vector<int> acc_root, acc_limbs, acc_off;
+    std::vector<int> agg_slot(n_aggs, -1);
     int accw = 0;
     for (int a = 0; a < n_aggs; a++) {
         out.agg_kind.push_back(aggs[a].kind);
@@ -892,9 +984,24 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         out.agg_scale.push_back(fr.scale);
         out.agg_acc_limbs.push_back(nacc);
         out.agg_acc_offset.push_back(acc_off[slot]);
+        agg_slot[a] = slot;
+    }
+    const int NR = (int)acc_root.size();
+    // Nullable columns take SQL's aggregate semantics (agg_sum_t on
+    // nullable_type, operators.hxx:1176-1193; COUNT of a nullable column
+    // counts its non-null rows, AriesEngineAlgorithm.h:725-736): a row adds to
+    // SUM/AVG of an expression only when none of that expression's columns is
+    // NULL, and every accumulator keeps its own count of those rows (two words
+    // per accumulator after a group's accumulators) for the SUM flag and the
+    // AVG divisor.  COUNT stays the group's row count (COUNT(*)).
+    bool any_nullable = false;
+    for (int c : used) any_nullable |= cols[c].nullable != 0;
+    std::vector<int> cnt_off;
+    if (any_nullable) {
+        for (int i = 0; i < NR; i++) cnt_off.push_back(accw + 2 * i);
+        accw += 2 * NR;
     }
     out.acc_words_per_group = accw;
-    const int NR = (int)acc_root.size();
 
     Emitter em(nodes, cols, f);
     em.plan(topo);
@@ -921,8 +1028,45 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         return d;
     };
     const int W = std::max(accw, 1);
+    std::vector<std::pair<std::string, std::string>> qval_calls;  // per accumulator: NULL test, arguments
 
     // generic kernel: blocks, indirection, nullable values; global accumulators
+    if (any_nullable) {
+        // one evaluation function per accumulated expression, over its own
+        // columns, so that a NULL in one expression's columns leaves the others
+        for (int i = 0; i < NR; i++) {
+            std::vector<int> sub;
+            std::vector<char> reach(n_nodes, 0);
+            reach[acc_root[i]] = 1;
+            for (auto it = topo.rbegin(); it != topo.rend(); ++it) {
+                if (!reach[*it]) continue;
+                const up_expr_node& nd = nodes[*it];
+                if (nd.left >= 0) reach[nd.left] = 1;
+                if (nd.right >= 0) reach[nd.right] = 1;
+            }
+            std::vector<int> sub_cols;
+            for (int k : topo)
+                if (reach[k]) {
+                    sub.push_back(k);
+                    if (nodes[k].kind == UP_NODE_COLUMN &&
+                        std::find(sub_cols.begin(), sub_cols.end(), nodes[k].column) == sub_cols.end())
+                        sub_cols.push_back(nodes[k].column);
+                }
+            std::sort(sub_cols.begin(), sub_cols.end());
+            Emitter ei(nodes, cols, f);
+            ei.plan(sub);
+            for (int k : sub) ei.node(k);
+            src << "UP_DI u32 up_qval" << i << "(" << params_decl(sub_cols) << "const bool words, u32 (&qv)["
+                << acc_limbs[i] << "]) {\n    u32 err = 0u;\n" << ei.constants() << ei.body.str();
+            src << "    to_twos(qv, v" << acc_root[i] << ", s" << acc_root[i] << ");\n    return err;\n}\n\n";
+            std::string null_test = "false", args;
+            for (int c : sub_cols) {
+                null_test += " || n" + std::to_string(c);
+                args += "in" + std::to_string(c) + ", ";
+            }
+            qval_calls.push_back({null_test, args});
+        }
+    }
     src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_query_acc(const UpQArgs a) {\n";
     src << "    u32 err = 0u;\n";
     src << "    const int ngr = q_groups(a);\n";
@@ -931,21 +1075,40 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     src << "    for (i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x; row < a.rows; row += stride) {\n";
     src << "        const int g = q_group(a, row);\n";
     src << "        if ((unsigned)g >= (unsigned)ngr) { err |= ERR_DOMAIN; continue; }\n";
-    src << "        atomicAdd(a.cnt + g, 1ull);\n";
-    src << "        bool isnull = false;\n";
-    for (int c : used) {
-        src << "        const u8* in" << c << " = col_ptr(a.col[" << c << "], row);\n";
-        src << "        if (in" << c << " == nullptr) isnull = true;\n";
-        if (cols[c].nullable)
-            src << "        else { if (in" << c << "[0] == 0) isnull = true; in" << c << " += 1; }\n";
+    if (any_nullable) {
+        // NULL: a nullable column's flag byte is 0, or a -1 row index
+        for (int c : used) {
+            src << "        const u8* in" << c << " = col_ptr(a.col[" << c << "], row);\n";
+            src << "        bool n" << c << " = in" << c << " == nullptr;\n";
+            if (cols[c].nullable)
+                src << "        if (!n" << c << ") { n" << c << " = in" << c << "[0] == 0; in" << c << " += 1; }\n";
+        }
+        src << "        atomicAdd(a.cnt + g, 1ull);\n";
+        for (int i = 0; i < NR; i++) {
+            src << "        if (!(" << qval_calls[i].first << ")) {\n";
+            src << "            u32 qv[" << acc_limbs[i] << "];\n";
+            src << "            err |= up_qval" << i << "(" << qval_calls[i].second << "false, qv);\n";
+            src << "            atomic_add_twos(a.acc + (i64)g * " << W << " + " << acc_off[i] << ", qv);\n";
+            src << "            const u32 one[2] = {1u, 0u};\n";
+            src << "            atomic_add_twos(a.acc + (i64)g * " << W << " + " << cnt_off[i] << ", one);\n";
+            src << "        }\n";
+        }
+    } else {
+        // a -1 row index on a column that is not nullable is outside the domain
+        src << "        bool isnull = false;\n";
+        for (int c : used) {
+            src << "        const u8* in" << c << " = col_ptr(a.col[" << c << "], row);\n";
+            src << "        if (in" << c << " == nullptr) isnull = true;\n";
+        }
+        src << "        if (isnull) { err |= ERR_DOMAIN; continue; }\n";
+        src << "        atomicAdd(a.cnt + g, 1ull);\n";
+        src << decl_t("        ");
+        src << "        err |= up_qvals(";
+        for (int c : used) src << "in" << c << ", ";
+        src << "false" << targs() << ");\n";
+        for (int i = 0; i < NR; i++)
+            src << "        atomic_add_twos(a.acc + (i64)g * " << W << " + " << acc_off[i] << ", qv" << i << ");\n";
     }
-    src << "        if (isnull) continue;\n";
-    src << decl_t("        ");
-    src << "        err |= up_qvals(";
-    for (int c : used) src << "in" << c << ", ";
-    src << "false" << targs() << ");\n";
-    for (int i = 0; i < NR; i++)
-        src << "        atomic_add_twos(a.acc + (i64)g * " << W << " + " << acc_off[i] << ", qv" << i << ");\n";
     src << "    }\n";
     src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
     src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n}\n\n";
@@ -962,7 +1125,7 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     for (int c : used) row_bytes += compact_bytes(cols[c].precision);
     int R = 1024;
     while (R > 128 && 2L * R * row_bytes > 32 * 1024) R /= 2;
-    const bool staged = 2L * R * row_bytes <= 32 * 1024;
+    const bool staged = 2L * R * row_bytes <= 32 * 1024 && !any_nullable;
     // register mode keeps per group a count and, per accumulator, its full
     // width when that is at most 4 limbs, else a 128-bit fast accumulator
     int reg_words = 1;
@@ -1191,6 +1354,9 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
             src << "        ((i64*)a.out[" << a << "])[g] = (i64)cnt;\n";
         } else {
             int n = out.agg_acc_limbs[a];
+            if (any_nullable)  // the accumulator's own count of non-NULL rows
+                src << "        const u64 cnt = (u64)acc[" << cnt_off[agg_slot[a]] << "] | ((u64)acc["
+                    << cnt_off[agg_slot[a]] + 1 << "] << 32);\n";
             src << "        u32 m[" << n << "];\n";
             src << "        for (int i = 0; i < " << n << "; i++) m[i] = acc[" << out.agg_acc_offset[a] << " + i];\n";
             src << "        const u32 neg = m[" << n - 1 << "] >> 31;\n";
@@ -1200,12 +1366,12 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
                 src << "        agg_image(img, cnt > 0 ? 1u : 0u, neg, " << out.agg_scale[a] << "u, m);\n";
             } else {
                 int nq = n + 1;
-                src << "        if (cnt == 0) { agg_image(img, 0u, 0u, " << out.agg_scale[a] + 4 << "u, m); }\n";
-                src << "        else {\n";
+                // a group without rows has a zero sum: the divide rule's zero-dividend case
+                src << "        {\n";
                 src << "            const u32 c2[2] = {(u32)cnt, (u32)(cnt >> 32)};\n";
                 src << "            u32 q[" << nq << "]; u32 sq;\n";
-                src << "            div_round<" << nq << ", " << n << ", 2, 1, 4u, 10000ull>(q, sq, m, neg, c2, 0u, P10_4);\n";
-                src << "            agg_image(img, 1u, sq, " << out.agg_scale[a] + 4 << "u, q);\n";
+                src << "            const u32 e = div_round<" << nq << ", " << n << ", 2, 1, 4u, 10000ull>(q, sq, m, neg, c2, 0u, P10_4);\n";
+                src << "            avg_image(img, cnt > 0 ? 1u : 0u, cnt, is_zero(m), sq, " << out.agg_scale[a] + 4 << "u, q, e);\n";
                 src << "        }\n";
             }
         }
@@ -1243,10 +1409,7 @@ namespace upi {
 namespace {
 const char* kBatchPrelude =
     "#define UP_MUL_UNROLL_PAIRS 1024\n"
-    "#include \"up_dev.cuh\"\nusing namespace up;\n"
-    "struct BTask { KCol col[8]; i64 rows; u8* out; const int* gid; u32* acc; u64* cnt; int n_groups; int words; };\n"
-    "struct BArgs { BTask* tasks; const int* item_task; const i64* item_tile; i64 n_items; "
-    "unsigned long long* head; u32* err; int tile_rows; int pad; };\n";
+    "#include \"up_dev.cuh\"\nusing namespace up;\n";  // BTask, BArgs: up_kargs.h
 
 uint64_t text_hash(const std::string& s) {
     uint64_t h = 1469598103934665603ull;
@@ -1364,11 +1527,10 @@ up_status generate_batch_module(const BatchTaskDesc* tasks, int n_tasks, Generat
                     src << "    agg_image(img, cnt > 0 ? 1u : 0u, neg, " << gt.agg_scale << "u, m);\n";
                 } else {
                     src << "    const u32 P10_4[1] = {10000u};\n";
-                    src << "    if (cnt == 0) { agg_image(img, 0u, 0u, " << gt.agg_scale + 4 << "u, m); return; }\n";
                     src << "    const u32 c2[2] = {(u32)cnt, (u32)(cnt >> 32)};\n";
                     src << "    u32 q[" << n + 1 << "]; u32 sq;\n";
-                    src << "    div_round<" << n + 1 << ", " << n << ", 2, 1, 4u, 10000ull>(q, sq, m, neg, c2, 0u, P10_4);\n";
-                    src << "    agg_image(img, 1u, sq, " << gt.agg_scale + 4 << "u, q);\n";
+                    src << "    const u32 e = div_round<" << n + 1 << ", " << n << ", 2, 1, 4u, 10000ull>(q, sq, m, neg, c2, 0u, P10_4);\n";
+                    src << "    avg_image(img, cnt > 0 ? 1u : 0u, cnt, is_zero(m), sq, " << gt.agg_scale + 4 << "u, q, e);\n";
                 }
             }
             src << "}\n";

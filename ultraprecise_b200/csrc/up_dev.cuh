@@ -18,6 +18,8 @@
 #ifndef UP_DEV_CUH_
 #define UP_DEV_CUH_
 
+#include "up_kargs.h"
+
 namespace up {
 
 typedef unsigned int u32;
@@ -226,12 +228,47 @@ UP_DI void shr_bits(u32 (&r)[N], const u32 (&a)[N], u32 s) {
 }
 
 // ------------------------------------------------------------ division
-// 2/1 division by a normalised 32-bit divisor with a precomputed reciprocal:
-// Moller & Granlund, "Improved division by invariant integers" (IEEE Trans.
-// Computers, 2011), Algorithm 4.  d has its top bit set, v = floor((2^64-1)/d)
-// - 2^32, and u1 < d; returns q = floor((u1*2^32 + u0)/d), r the remainder.
-UP_DI u32 reciprocal_u32(u32 d) { return (u32)(0xffffffffffffffffull / d); }
+// Integer division runs its quotient-digit estimates on the FP64 pipe (idle
+// in these kernels) instead of 64-bit integer divides, which the GPU has no
+// instruction for: each estimate is a few double operations and is then made
+// exact by integer multiply-subtract and at most one correction.
 
+// Exact double of a 32-bit value without a conversion instruction: the
+// value's bits as the mantissa of 2^52 + x, minus 2^52 (exact).
+UP_DI double u32_to_f64(u32 x) { return __dadd_rn(__hiloint2double(0x43300000, (int)x), -4503599627370496.0); }
+
+// floor(e) for 0 <= e < 2^32, or 0xffffffff when floor(e) >= 2^32: adding
+// 2^52 rounded toward -inf leaves floor(e) in the low mantissa bits.
+UP_DI u32 f64_floor_u32_sat(double e) {
+    const double y = __dadd_rd(e, 4503599627370496.0);
+    return __double2hiint(y) == 0x43300000 ? (u32)__double2loint(y) : 0xffffffffu;
+}
+
+// Reciprocal of a normalised divisor d (top bit set) for the 2/1 division of
+// Moller & Granlund, "Improved division by invariant integers" (IEEE Trans.
+// Computers, 2011): v = floor((2^64 - 1) / d) - 2^32.  The double estimate
+// 2^64/d - 2^32 is within 2^-19 of the exact quotient; taking one less and
+// stepping up while (2^32 + v + 1) * d < 2^64 makes it exact in at most two
+// steps.
+UP_DI u32 reciprocal_u32(u32 d) {
+    const double r = __drcp_rn(u32_to_f64(d));                      // 1/d, correctly rounded
+    const double e = __fma_rn(r, 18446744073709551616.0, -4294967296.0);  // ~ 2^64/d - 2^32, in [0, 2^32]
+    u32 v = f64_floor_u32_sat(e);
+    v = v ? v - 1u : 0u;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        // (2^32 + v + 1) * d = d * 2^32 + (v + 1) * d; below 2^64 when the sum does not carry
+        const u64 lo = (u64)(v + 1u) * d;
+        const u64 hi = (u64)d << 32;
+        const bool below = v != 0xffffffffu && lo + hi >= hi;
+        v += below ? 1u : 0u;
+    }
+    return v;
+}
+
+// 2/1 division by a normalised 32-bit divisor with its reciprocal v (Moller
+// & Granlund 2011, Algorithm 4); u1 < d; returns floor((u1*2^32 + u0)/d) and
+// the remainder in r.
 UP_DI u32 div2by1(u32 u1, u32 u0, u32 d, u32 v, u32& r) {
     u64 q = (u64)v * u1;
     q += ((u64)u1 << 32) | u0;
@@ -250,12 +287,62 @@ UP_DI u32 div2by1(u32 u1, u32 u0, u32 d, u32 v, u32& r) {
     return q1;
 }
 
+// Quotient digits of Knuth's Algorithm D from the FP64 pipe.  With the
+// divisor normalised (its top limb vtop has the top bit set) and the current
+// remainder window w[0..n] < divisor * 2^32, the digit is
+// floor(window / divisor) < 2^32.  The estimate is (w[n]:w[n-1]) * 2^32 /
+// (vtop:vnext) in doubles: its relative error is below 2^-51 (four roundings)
+// and the limbs it leaves out move it by less than 2^-31, so it is within
+// 2^-18.9 of the exact quotient; biased up by 2^-18 and floored it is the
+// digit or the digit + 1, which Algorithm D's add-back corrects.
+struct QuotEst {
+    double rcp;  // 2^32 / (vtop:vnext), correctly rounded
+    UP_DI void init(u32 vtop, u32 vnext) {
+        const double vd = __fma_rn(u32_to_f64(vtop), 4294967296.0, u32_to_f64(vnext));
+        rcp = __dmul_rn(__drcp_rn(vd), 4294967296.0);
+    }
+    UP_DI u32 digit(u32 u1, u32 u0) const {
+        const double t = __fma_rn(u32_to_f64(u1), 4294967296.0, u32_to_f64(u0));
+        return f64_floor_u32_sat(__fma_rn(t, rcp, 3.814697265625e-06));  // + 2^-18
+    }
+};
+
+// One step of Algorithm D on the window w[0..NB]: subtract qhat * bn, add
+// back once when qhat was one too large; returns the digit.
+template <int NB>
+UP_DI u32 knuth_step(u32 (&w)[NB + 1], const u32 (&bn)[NB], u32 qhat) {
+    u64 carry = 0;
+    i64 borrow = 0;
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+        const u64 p = (u64)qhat * bn[i] + carry;
+        carry = p >> 32;
+        const i64 t = (i64)w[i] - (i64)(u32)p + borrow;
+        w[i] = (u32)t;
+        borrow = t >> 32;  // 0 or -1
+    }
+    const i64 t = (i64)w[NB] - (i64)carry + borrow;
+    w[NB] = (u32)t;
+    if (t < 0) {
+        qhat--;
+        u64 c = 0;
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            c += (u64)w[i] + bn[i];
+            w[i] = (u32)c;
+            c >>= 32;
+        }
+        w[NB] += (u32)c;
+    }
+    return qhat;
+}
+
 // Knuth, TAOCP vol. 2, 4.3.1, Algorithm D in base 2^32 with static array
 // sizes: the divisor is normalised to exactly NB limbs (top bit set) by a
-// dynamic left shift applied to both operands; quotient steps above the
-// dividend's actual length are skipped (their digits are zero).  Quotient
-// digit estimates use the 2/1 reciprocal division above.
-// q = floor(x / b), rem = x mod b.  Requires b != 0.
+// dynamic left shift applied to both operands; the nx - nb + 1 quotient
+// digits that can be nonzero are produced (nx, nb: the operands' significant
+// limbs), each estimated by QuotEst.  q = floor(x / b), rem = x mod b.
+// Requires b != 0.
 template <int NX, int NB>
 UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&b)[NB]) {
     if constexpr (NB == 1) {
@@ -270,6 +357,7 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
         }
         rem[0] = r >> sh;
     } else {
+    // the shift reaches past a limb when b's value is narrower than NB limbs
     constexpr int NU = NX + NB + 1;
     const u32 bl = bitlen(b);
     const u32 s = 32u * NB - bl;  // normalising shift
@@ -281,66 +369,28 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
         copy_ext(xe, x);
         shl_bits(un, xe, s);
     }
-    const u32 vtop = bn[NB - 1];
-    const u32 vnext = bn[NB - 2];
-    const u32 vinv = reciprocal_u32(vtop);
-    // quotient digits above nx - nb + 1 are zero (x < 2^(32 nx), b >= 2^(32 (nb-1)))
-    const int jmax = (int)((bitlen(x) + 31u) >> 5) - (int)((bl + 31u) >> 5) + 1;
+    QuotEst est;
+    est.init(bn[NB - 1], bn[NB - 2]);
+    // digits j = jmax .. 0 with jmax = nx - nb; the window of digit j is un[j .. j+NB]
+    const int jmax = (int)((bitlen(x) + 31u) >> 5) - (int)((bl + 31u) >> 5);
+#pragma unroll
+    for (int i = 0; i < NX; i++) q[i] = 0u;
+    if (jmax < 0) {  // x < b
+        copy_ext(rem, x);
+        return;
+    }
     constexpr bool kUnroll = (NX + 1) * NB <= 96;
     if constexpr (!kUnroll && NB <= 40) {
         // Wide operands: the rolled loop keeps the current remainder window
-        // un[j .. j+NB] in registers (static indices) and moves it up one limb
-        // per quotient digit, reading a single dividend limb per step, instead
-        // of addressing un[i + j] in local memory 2*NB times per step.  Up to
-        // 40-limb divisors (measured on B200: 1.1x faster at 32 limbs; at 63
-        // limbs window and divisor no longer fit the registers and it is 1.8x
-        // slower).
-#pragma unroll
-        for (int i = 0; i < NX; i++) q[i] = 0u;
-        const int j0 = jmax < NX ? jmax : NX;
+        // un[j .. j+NB] in registers (static indices) and moves it down one
+        // limb per quotient digit, reading a single dividend limb per step.
         u32 w[NB + 1];
 #pragma unroll
-        for (int i = 0; i <= NB; i++) w[i] = j0 >= 0 ? un[j0 + i] : 0u;
+        for (int i = 0; i <= NB; i++) w[i] = un[jmax + i];
 #pragma unroll 1
-        for (int j = j0; j >= 0; j--) {
-            const u32 u1 = w[NB], u0 = w[NB - 1];
-            u64 qhat, rhat;
-            if (u1 >= vtop) {
-                qhat = 0xffffffffull;
-                rhat = (u64)u0 + vtop;
-            } else {
-                u32 r32;
-                qhat = div2by1(u1, u0, vtop, vinv, r32);
-                rhat = r32;
-            }
-            while ((rhat >> 32) == 0u && qhat * vnext > ((rhat << 32) | w[NB - 2])) {
-                qhat--;
-                rhat += vtop;
-            }
-            u64 carry = 0;
-            i64 borrow = 0;
-#pragma unroll
-            for (int i = 0; i < NB; i++) {
-                const u64 p = qhat * bn[i] + carry;
-                carry = p >> 32;
-                const i64 t = (i64)w[i] - (i64)(u32)p - borrow;
-                w[i] = (u32)t;
-                borrow = t < 0 ? 1 : 0;
-            }
-            const i64 t = (i64)w[NB] - (i64)carry - borrow;
-            w[NB] = (u32)t;
-            if (t < 0) {
-                qhat--;
-                u64 c = 0;
-#pragma unroll
-                for (int i = 0; i < NB; i++) {
-                    c += (u64)w[i] + bn[i];
-                    w[i] = (u32)c;
-                    c >>= 32;
-                }
-                w[NB] += (u32)c;
-            }
-            if (j < NX) q[j < NX ? j : 0] = (u32)qhat;
+        for (int j = jmax; j >= 0; j--) {
+            const u32 qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+            if (j < NX) q[j < NX ? j : 0] = qd;
             if (j > 0) {
 #pragma unroll
                 for (int i = NB; i > 0; i--) w[i] = w[i - 1];
@@ -349,55 +399,21 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
         }
         u32 rl[NB];
 #pragma unroll
-        for (int i = 0; i < NB; i++) rl[i] = j0 >= 0 ? w[i] : un[i];
+        for (int i = 0; i < NB; i++) rl[i] = w[i];
         shr_bits(rem, rl, s);
         return;
     }
-#pragma unroll(kUnroll ? NX + 1 : 1)
-    for (int j = NX; j >= 0; j--) {
-        if (j > jmax) {
-            if (j < NX) q[j < NX ? j : 0] = 0u;
-            continue;
-        }
-        const u32 u1 = un[j + NB], u0 = un[j + NB - 1];
-        u64 qhat, rhat;
-        if (u1 >= vtop) {
-            qhat = 0xffffffffull;
-            rhat = (u64)u0 + vtop;
-        } else {
-            u32 r32;
-            qhat = div2by1(u1, u0, vtop, vinv, r32);
-            rhat = r32;
-        }
-        while ((rhat >> 32) == 0u && qhat * vnext > ((rhat << 32) | un[j + NB - 2])) {
-            qhat--;
-            rhat += vtop;
-        }
-        // multiply and subtract qhat * bn from un[j .. j+NB]
-        u64 carry = 0;
-        i64 borrow = 0;
+    // Static window positions: digit j uses un[j .. j+NB], j <= jmax <= NX - 1.
+#pragma unroll(kUnroll ? NX : 1)
+    for (int j = NX - 1; j >= 0; j--) {
+        if (j > jmax) continue;
+        u32 w[NB + 1];
 #pragma unroll
-        for (int i = 0; i < NB; i++) {
-            u64 p = qhat * bn[i] + carry;
-            carry = p >> 32;
-            i64 t = (i64)un[i + j] - (i64)(u32)p - borrow;
-            un[i + j] = (u32)t;
-            borrow = t < 0 ? 1 : 0;
-        }
-        i64 t = (i64)un[j + NB] - (i64)carry - borrow;
-        un[j + NB] = (u32)t;
-        if (t < 0) {
-            qhat--;
-            u64 c = 0;
+        for (int i = 0; i <= NB; i++) w[i] = un[j + i];
+        const u32 qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
-            for (int i = 0; i < NB; i++) {
-                c += (u64)un[i + j] + bn[i];
-                un[i + j] = (u32)c;
-                c >>= 32;
-            }
-            un[j + NB] += (u32)c;
-        }
-        if (j < NX) q[j < NX ? j : 0] = (u32)qhat;
+        for (int i = 0; i <= NB; i++) un[j + i] = w[i];
+        q[j] = qd;
     }
     u32 rl[NB];
 #pragma unroll
@@ -626,6 +642,7 @@ UP_DI u32 st_compact_words(u8* p, const u32 (&m)[N], u32 sign) {
     return compact_overflow<B>(m);
 }
 
+#ifndef UP_HOST_TEST  // the host build of the arithmetic (CPU tests) stops here
 // ------------------------------------------------ cooperative values
 // T threads (T a power of two dividing 32; a group is T consecutive lanes of
 // one warp) hold one value: the thread of rank g holds limbs [g*K, g*K + K).
@@ -1256,17 +1273,11 @@ UP_DI u32 tpi_st(u8* __restrict__ p, const u32 (&x)[K], u32 sign, bool store) {
     return tpi_ballot<T>(over) ? ERR_OVERFLOW : 0u;
 }
 
+#endif  // UP_HOST_TEST
 // ------------------------------------------------------ column access
 // Per-column kernel argument: the AriesColumnDataIterator shape
 // (AriesColumnDataIterator.hxx:8-41).
-struct KCol {
-    const u8* data;
-    const u8* const* blocks;
-    const i64* prefix;
-    const int* indices;
-    int n_blocks;
-    int value_bytes;
-};
+typedef ::UpKCol KCol;  // up_kargs.h
 
 // Row -> value pointer for the block/indirection path
 // (AriesColumnDataIterator::operator[], AriesColumnDataIterator.cu:60-115).
@@ -1410,6 +1421,21 @@ UP_DI void agg_image(u8* img, u32 flag, u32 sign, u32 frac, const u32 (&m)[N]) {
     }
 }
 
+// The AVG image: the nullable SUM divided by its int64 count the way
+// nullable_type<Decimal>::operator/=(int64_t) does (aries_types.hxx:626-631 ->
+// Decimal::DivOrMod, decimal.cu:2200-2228): the flag survives only a nonzero
+// count; a zero dividend gives +0 with prec = frac + 1 (frac already raised by
+// 4); a zero count with a nonzero dividend keeps the dividend and sets error
+// ERR_DIV_BY_ZERO (2).  q, sign, err: the div_round result for the dividend.
+template <int N>
+UP_DI void avg_image(u8* img, u32 sum_flag, u64 count, bool dividend_zero, u32 sign, u32 frac,
+                     const u32 (&q)[N], u32 err) {
+    agg_image(img, (sum_flag && count != 0ull) ? 1u : 0u, dividend_zero ? 0u : sign, frac, q);
+    if (dividend_zero) img[2] = (u8)(frac + 1u);
+    img[4] = (err & ERR_DIV0) ? 2 : 0;
+}
+
+#ifndef UP_HOST_TEST
 // ------------------------------------------------- bulk-copy pipeline
 // 1-D bulk copies (cp.async.bulk, the TMA engine without a tensor map) between
 // global and shared memory, completed through an mbarrier.  Sizes are
@@ -1442,11 +1468,11 @@ UP_DI void bulk_load(void* dst_smem, const void* src_gmem, u32 bytes, u64* bar) 
         : "memory");
 }
 
-// Wait for the mbarrier phase with the given parity; gives up after a bounded
-// number of polls and returns false (the caller records ERR_TIMEOUT).
-UP_DI bool mbar_wait(u64* bar, u32 parity) {
+// Wait for the mbarrier phase with the given parity; gives up after `polls`
+// polls and returns false (the caller records ERR_TIMEOUT).
+UP_DI bool mbar_wait(u64* bar, u32 parity, u32 polls = 1u << 24) {
     const u32 a = smem_addr(bar);
-    for (u32 it = 0; it < (1u << 24); it++) {
+    for (u32 it = 0; it < polls; it++) {
         u32 done;
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -1469,6 +1495,7 @@ UP_DI void bulk_store(void* dst_gmem, const void* src_smem, u32 bytes) {
 UP_DI void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 UP_DI void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 UP_DI void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+#endif  // UP_HOST_TEST
 
 }  // namespace up
 

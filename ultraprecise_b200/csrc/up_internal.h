@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/ultraprecise.h"
+#include "up_kargs.h"
 
 namespace upi {
 
@@ -56,6 +57,17 @@ struct NodeFacts {
 up_status analyze_nodes(const up_expr_node* nodes, int n_nodes, const up_col_type* cols, int n_cols,
                         std::vector<NodeFacts>& facts, std::vector<int>& topo, const std::vector<int>& roots);
 int limbs_for_bits(int bits);
+// Cost-model features of an expression launch (ultraprecise_costmodel.h).
+up_status expr_cost_features(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols, int n_cols,
+                             int tpv, int64_t rows, float* out, bool* coop_ok);
+// The process-wide model up_module_compile consults for automatic threads per
+// value (NULL: the width rule); set by up_costmodel_set_default.
+struct CostChoice {
+    bool valid = false;
+    int tpv = 1;
+};
+CostChoice default_model_choose_tpv(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
+                                    int n_cols);
 
 // ------------------------------------------------------------ code generation
 struct GeneratedModule {
@@ -79,6 +91,9 @@ struct GeneratedModule {
     int q_smem = 0;               // dynamic shared memory of the tile kernels
     long work_per_row = 0;        // limb-product work + bytes per row (scheduling cost estimate)
     int threads_per_value = 1;    // threads cooperating on one value in the tile kernel
+    // up_expr_multi (merged launches of several requests): rows per virtual
+    // tile (0: the module has no such kernel), CTA threads, shared memory
+    int multi_rows = 0, multi_threads = 0, multi_smem = 0;
 };
 up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
                                int n_cols, const up_compile_opts* opts, GeneratedModule& out);
@@ -200,8 +215,14 @@ struct QueryKeys {
     // 131072) and may be at most `capacity`, which sizes the accumulators
     int capacity = 0;
 };
+// Scratch of a query launch for n_groups groups: the accumulators (16-byte
+// padded) followed by one int64 count per group.
+size_t query_scratch_bytes(const upi::GeneratedModule& g, int32_t n_groups);
+// scratch: caller-provided device memory of scratch_bytes (at least
+// query_scratch_bytes, 16-byte aligned) used instead of a stream-ordered
+// allocation; the launch clears what it uses on `stream`.
 up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_t rows, const int32_t* group_ids,
                           int32_t n_groups, void* const* outs, uint32_t* err_word, void* stream, bool spread,
-                          const QueryKeys* keys = nullptr);
+                          const QueryKeys* keys = nullptr, void* scratch = nullptr, size_t scratch_bytes = 0);
 
 #endif  // UP_INTERNAL_H_

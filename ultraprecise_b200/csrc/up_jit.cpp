@@ -27,14 +27,21 @@
 #include <thread>
 #include <unordered_map>
 
+#include <zlib.h>
+
 #include "up_internal.h"
 
 namespace upi {
 
-#include "up_dev_embed.inc"  // defines kUpDevCuh (the text of up_dev.cuh)
+#include "up_dev_embed.inc"  // defines kUpDevCuh and kUpKargsH (the texts of up_dev.cuh and up_kargs.h)
 
 const std::string& device_header_source() {
     static const std::string s(kUpDevCuh);
+    return s;
+}
+
+const std::string& kargs_header_source() {
+    static const std::string s(kUpKargsH);
     return s;
 }
 
@@ -105,20 +112,35 @@ std::string full_key(const std::string& src, bool rdc) {
     nvrtcVersion(&maj, &min);
     static const std::string hdr_hash = [] {
         char b[40];
-        snprintf(b, sizeof b, "%016llx", (unsigned long long)fnv1a(device_header_source()));
+        snprintf(b, sizeof b, "%016llx", (unsigned long long)fnv1a(device_header_source() + kargs_header_source()));
         return std::string(b);
     }();
     return std::string(kArch) + (rdc ? "|rdc" : "") + "|nvrtc" + std::to_string(maj) + "." + std::to_string(min) +
            "|hdr" + hdr_hash + "|" + src;
 }
 
-bool read_file(const std::string& p, std::string& out) {
+bool read_file_plain(const std::string& p, std::string& out) {
     std::ifstream f(p, std::ios::binary);
     if (!f) return false;
     std::ostringstream o;
     o << f.rdbuf();
     out = o.str();
     return true;
+}
+
+// A cache file, or its gzip-compressed form `p.gz` (the in-tree cache that
+// travels with the library is stored compressed).
+bool read_file(const std::string& p, std::string& out) {
+    if (read_file_plain(p, out)) return true;
+    gzFile z = gzopen((p + ".gz").c_str(), "rb");
+    if (!z) return false;
+    out.clear();
+    char buf[1 << 16];
+    int n;
+    while ((n = gzread(z, buf, sizeof buf)) > 0) out.append(buf, (size_t)n);
+    const bool ok = n == 0;
+    gzclose(z);
+    return ok;
 }
 
 void write_file_atomic(const std::string& p, const std::string& data) {
@@ -153,9 +175,9 @@ bool cache_lookup(const std::string& name, const std::string& key, std::string& 
 
 up_status nvrtc_compile(const std::string& src, std::vector<char>& cubin, std::string& log, bool rdc) {
     nvrtcProgram prog;
-    const char* hdr_src[1] = {device_header_source().c_str()};
-    const char* hdr_name[1] = {"up_dev.cuh"};
-    nvrtcResult r = nvrtcCreateProgram(&prog, src.c_str(), "up_kernel.cu", 1, hdr_src, hdr_name);
+    const char* hdr_src[2] = {device_header_source().c_str(), kargs_header_source().c_str()};
+    const char* hdr_name[2] = {"up_dev.cuh", "up_kargs.h"};
+    nvrtcResult r = nvrtcCreateProgram(&prog, src.c_str(), "up_kernel.cu", 2, hdr_src, hdr_name);
     if (r != NVRTC_SUCCESS) return fail(UP_ERR_COMPILE, std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r));
     // UP_JIT_VERBOSE=1 adds ptxas's resource report (registers, spills,
     // shared memory per kernel) and prints the compile log to stderr.

@@ -64,8 +64,7 @@ __global__ void k_division_int64(const u8* __restrict__ sums, const int64_t* __r
     u32 sq;
     const u32 err = up::div_round<34, 32, 2, 1, 4u, 10000ull>(q, sq, m, sign, c2, 0u, p10);
     u8* o = out + (int64_t)i * UP_AGG_DECIMAL_BYTES;
-    up::agg_image(o, img[0], sq, (u32)img[3] + 4u, q);
-    o[4] = (err & up::ERR_DIV0) ? 2 : 0;  // Decimal::error = ERR_DIV_BY_ZERO (decimal.hxx:28)
+    up::avg_image(o, img[0], cnt, up::is_zero(m), sq, (u32)img[3] + 4u, q, err);
 }
 
 cudaError_t launch_division_int64(const uint8_t* sums, const int64_t* counts, int32_t n, uint8_t* out,
@@ -363,22 +362,23 @@ __global__ void k_flush(uint4* __restrict__ buf, int64_t n, u32 salt) {
         buf[i] = make_uint4(salt, (u32)i, salt ^ 1u, (u32)(i >> 32));
 }
 
-// Independent 32x32+64 multiply-adds: 8 chains per thread, no dependency
-// between chains, one dependency per chain per iteration.
+// The limb multiply-add (32 x 32 -> 64 plus a 64-bit addend, one wide
+// integer multiply-add instruction) at full rate: 8 independent chains per
+// thread and nothing else in the loop.  Each step multiplies by the high word
+// of its own accumulator, so the recurrence is not affine (the loop cannot be
+// folded into a closed form) and needs no instruction besides the
+// multiply-add itself.
 __global__ void __launch_bounds__(256) k_imad(u64* __restrict__ sink, int iters, u32 seed) {
     u32 x[8];
     u64 acc[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-        x[k] = seed * (threadIdx.x + 1u) + 977u * k;
-        acc[k] = k;
+        x[k] = (seed * (threadIdx.x + 1u) + 977u * k) | 1u;
+        acc[k] = ((u64)(seed + k) << 32) | (threadIdx.x * 31u + k);
     }
-    const u32 y = seed ^ 0x9e3779b9u;
     for (int it = 0; it < iters; it++) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) acc[k] = (u64)x[k] * y + acc[k];
-#pragma unroll
-        for (int k = 0; k < 8; k++) x[k] ^= (u32)acc[k];
+        for (int k = 0; k < 8; k++) acc[k] = (u64)x[k] * (u32)(acc[k] >> 32) + acc[k];
     }
     u64 s = 0;
 #pragma unroll
@@ -386,11 +386,42 @@ __global__ void __launch_bounds__(256) k_imad(u64* __restrict__ sink, int iters,
     if (s == 0x123456789ull) sink[0] = s;
 }
 
+// The bounded wait of the bulk-copy pipelines, made to run out: an mbarrier
+// armed for `bytes` of transfer that nothing ever sends (no copy is issued),
+// waited on with `polls` polls by the same code the tile kernels use; the
+// timeout is reported the way they report it (ERR_TIMEOUT in the error word).
+// Nothing is left in flight: the barrier lives in this block's shared memory.
+__global__ void k_wait_timeout_probe(u32 polls, u32 bytes, u32* __restrict__ err_word,
+                                     u32* __restrict__ done_word) {
+    __shared__ __align__(8) u64 bar;
+    if (threadIdx.x == 0) {
+        up::mbar_init(&bar, 1);
+        up::mbar_init_fence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) up::mbar_expect_tx(&bar, bytes);
+    __syncthreads();
+    const bool ok = up::mbar_wait(&bar, 0u, polls);
+    const bool all_timed_out = __syncthreads_and(!ok);
+    if (threadIdx.x == 0) {
+        if (all_timed_out) atomicOr(err_word, up::ERR_TIMEOUT);
+        atomicAdd(done_word, 1u);
+    }
+}
+
 }  // namespace upi
 
 using namespace upi;
 
 extern "C" {
+
+up_status up_util_wait_timeout_probe(uint32_t polls, uint32_t* err_word, uint32_t* done_word, void* stream) {
+    if (!err_word || !done_word) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    if (polls == 0 || polls > (1u << 24)) return fail(UP_ERR_INVALID_ARG, "polls must be 1 .. 2^24");
+    k_wait_timeout_probe<<<1, 32, 0, (cudaStream_t)stream>>>(polls, 256u, err_word, done_word);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? UP_OK : fail(UP_ERR_CUDA, cudaGetErrorString(e));
+}
 
 up_status up_util_gen_digits(void* out, int64_t rows, int32_t precision, uint64_t seed, int32_t signed_,
                              int32_t nonzero, void* stream) {

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -67,6 +68,7 @@ struct up_serve {
     int64_t budget = 0, outstanding = 0, max_outstanding = 0;
     int32_t inflight = 0, max_inflight_seen = 0;
     int64_t submitted = 0, completed = 0, failed = 0, deferred = 0;
+    std::atomic<int64_t> merged_launches{0}, merged_requests{0};
     std::vector<double> lat;           // completed since the last stats reset
 
     double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
@@ -157,6 +159,81 @@ void launch(up_serve* s, Req* r) {
     }
 }
 
+// Launch requests of one expression module as one merged kernel on the
+// first request's stream (scheduler thread, lock not held).
+void launch_merged(up_serve* s, std::vector<Req*>& g) {
+    cudaStream_t st = g[0]->stream;
+    std::vector<up_column> in;
+    std::vector<int64_t> rows;
+    std::vector<void*> outs;
+    std::vector<uint32_t*> errs;
+    std::vector<Req*> ok;
+    for (Req* r : g) {
+        r->stream = st;
+        cudaError_t e = cudaMallocAsync(&r->mem, (size_t)r->out_bytes, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(r->mem, 0, 4, st);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            r->mem = nullptr;
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->state = UP_REQ_FAILED;
+            r->done_ms = s->now_ms();
+            s->inflight--;
+            s->failed++;
+            s->done_cv.notify_all();
+            continue;
+        }
+        in.insert(in.end(), r->in.begin(), r->in.end());
+        rows.push_back(r->rows);
+        outs.push_back((uint8_t*)r->mem + r->part_off[0]);
+        errs.push_back((uint32_t*)r->mem);
+        ok.push_back(r);
+    }
+    if (ok.empty()) return;
+    const int n_in = (int)ok[0]->in.size();
+    up_status status = up_expr_launch_many(ok[0]->module, in.data(), n_in, rows.data(), (int32_t)ok.size(),
+                                           outs.data(), errs.data(), st);
+    s->merged_launches++;
+    s->merged_requests += (int64_t)ok.size();
+    for (Req* r : ok) {
+        cudaError_t e = status == UP_OK ? cudaMemcpyAsync(r->host_err, r->mem, 4, cudaMemcpyDeviceToHost, st)
+                                        : cudaErrorUnknown;
+        if (e == cudaSuccess) e = cudaLaunchHostFunc(st, on_done, r);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->state = UP_REQ_FAILED;
+            r->done_ms = s->now_ms();
+            s->inflight--;
+            s->failed++;
+            s->done_cv.notify_all();
+        }
+    }
+}
+
+// Same-module expression requests of one dispatch (at least two, contiguous
+// columns, not heavy) become merged launches; the rest launch one by one.
+void dispatch(up_serve* s, std::vector<Req*>& batch) {
+    if (!s->opts.merge) {
+        for (Req* r : batch) launch(s, r);
+        return;
+    }
+    std::unordered_map<up_module*, std::vector<Req*>> by_mod;
+    std::vector<Req*> single;
+    for (Req* r : batch) {
+        bool mergeable = !r->module->is_query && !r->heavy && r->rows > 0 && r->module->jm.gen.multi_rows > 0;
+        for (const up_column& c : r->in)
+            mergeable = mergeable && c.data && c.n_blocks <= 0 && !c.indices && !c.nullable;
+        if (mergeable) by_mod[r->module].push_back(r);
+        else single.push_back(r);
+    }
+    for (auto& kv : by_mod) {
+        if (kv.second.size() >= 2) launch_merged(s, kv.second);
+        else single.push_back(kv.second[0]);
+    }
+    for (Req* r : single) launch(s, r);
+}
+
 void scheduler(up_serve* s) {
     cudaSetDevice(s->device);
     std::vector<Req*> batch;
@@ -165,6 +242,7 @@ void scheduler(up_serve* s) {
         {
             std::unique_lock<std::mutex> lk(s->mu);
             bool waited_for_memory = false;
+            bool window_used = false;
             for (;;) {
                 if (s->stop) return;
                 // admit in arrival order while memory and the in-flight cap allow
@@ -189,12 +267,21 @@ void scheduler(up_serve* s) {
                                          : s->streams[s->next_stream++ % s->streams.size()];
                     r->state = UP_REQ_RUNNING;
                     batch.push_back(r);
+                    if ((int)batch.size() >= s->opts.max_batch) break;
                 }
-                if (!batch.empty()) break;
+                if (!batch.empty()) {
+                    // continuous batching window: wait a little for more arrivals to admit with these
+                    if (s->opts.batch_window_us > 0 && (int)batch.size() < s->opts.max_batch && !window_used) {
+                        window_used = true;
+                        s->cv.wait_for(lk, std::chrono::duration<double, std::micro>(s->opts.batch_window_us));
+                        continue;
+                    }
+                    break;
+                }
                 s->cv.wait(lk);
             }
         }
-        for (Req* r : batch) launch(s, r);
+        dispatch(s, batch);
     }
 }
 
@@ -210,6 +297,7 @@ up_status up_serve_create(const up_serve_opts* opts, up_serve** out) {
     if (s->opts.n_streams <= 0) s->opts.n_streams = 8;
     if (s->opts.max_inflight <= 0) s->opts.max_inflight = 1024;
     if (s->opts.reserve_bytes <= 0) s->opts.reserve_bytes = 2ll << 30;
+    if (s->opts.max_batch <= 0) s->opts.max_batch = 256;
     cudaError_t e = cudaGetDevice(&s->device);
     size_t fr = 0, tot = 0;
     if (e == cudaSuccess) e = cudaMemGetInfo(&fr, &tot);
@@ -350,6 +438,8 @@ up_status up_serve_stats_get(up_serve* s, int32_t reset, up_serve_stats* out) {
         out->max_outstanding_bytes = s->max_outstanding;
         out->budget_bytes = s->budget;
         out->max_inflight_seen = s->max_inflight_seen;
+        out->merged_launches = s->merged_launches.load();
+        out->merged_requests = s->merged_requests.load();
         v = s->lat;
         if (reset) {
             s->lat.clear();

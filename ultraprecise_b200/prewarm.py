@@ -84,6 +84,43 @@ def prewarm(verbose: bool = False) -> None:
         list(ex.map(lambda c: compile_expr_only(c[2], c[3], c[4]), workloads.coop_cases()))
     if verbose:
         print("prewarmed cooperative cases")
+    prewarm_costmodel(workers)
+    if verbose:
+        print("prewarmed cost-model shapes")
+
+
+def prewarm_costmodel(workers: int = 8) -> None:
+    """Every cost-model training and held-out shape at every threads per value
+    (the launches the model is trained and judged on)."""
+    import concurrent.futures as cf
+    shapes = workloads.costmodel_train_shapes() + workloads.costmodel_eval_shapes()
+    jobs = [(e, cols, t) for _, e, cols in shapes for t in (1, 2, 4, 8, 16, 32)]
+    with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+        list(ex.map(lambda j: compile_expr_only(*j), jobs))
+
+
+def compress(verbose: bool = False) -> None:
+    """Store the in-tree cache gzip-compressed (the JIT reads `<entry>.gz`
+    when the plain file is absent), so the library and its prebuilt kernels
+    stay small enough to travel."""
+    import gzip
+    import os
+    from . import build as B
+    cache = os.path.join(os.path.dirname(os.path.abspath(B.__file__)), "_jitcache")
+    before = after = 0
+    for name in sorted(os.listdir(cache)):
+        if not (name.endswith(".cubin") or name.endswith(".key")):
+            continue
+        path = os.path.join(cache, name)
+        data = open(path, "rb").read()
+        with gzip.open(path + ".gz.tmp", "wb", compresslevel=6) as f:
+            f.write(data)
+        os.replace(path + ".gz.tmp", path + ".gz")
+        os.remove(path)
+        before += len(data)
+        after += os.path.getsize(path + ".gz")
+    if verbose:
+        print(f"compressed cache: {before / 1e6:.1f} MB -> {after / 1e6:.1f} MB")
 
 
 def prune(verbose: bool = False) -> None:
@@ -108,5 +145,7 @@ if __name__ == "__main__":
     import sys
     if "--prune" in sys.argv:
         prune(verbose="-v" in sys.argv)
+    elif "--compress" in sys.argv:
+        compress(verbose=True)
     else:
         prewarm(verbose=True)

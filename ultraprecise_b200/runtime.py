@@ -24,11 +24,31 @@ def _stream_ptr(stream) -> int:
 @dataclass
 class DeviceColumn:
     """A compact decimal column in HBM: rows x value_bytes uint8."""
-    data: torch.Tensor
+    data: torch.Tensor | None
     precision: int
     scale: int
     nullable: bool = False
     indices: torch.Tensor | None = None   # int32 row indirection (-1 = NULL)
+    # block list (the reference's multi-block AriesColumnDataIterator): the
+    # rows live in several device buffers; block_ptrs holds their addresses
+    # and block_prefix the int64 row prefix sums (n_blocks + 1), both on the
+    # device, and blocks keeps the buffers alive
+    blocks: list | None = None
+    block_ptrs: torch.Tensor | None = None
+    block_prefix: torch.Tensor | None = None
+
+    @staticmethod
+    def from_blocks(blocks, precision: int, scale: int, nullable: bool = False) -> "DeviceColumn":
+        """A column whose rows are spread over several device buffers (uint8
+        tensors of whole values), in order."""
+        vb = codec.compact_bytes(precision) + (1 if nullable else 0)
+        counts = [b.numel() // vb for b in blocks]
+        prefix = [0]
+        for n in counts:
+            prefix.append(prefix[-1] + n)
+        ptrs = torch.tensor([b.data_ptr() for b in blocks], dtype=torch.int64, device="cuda")
+        pre = torch.tensor(prefix, dtype=torch.int64, device="cuda")
+        return DeviceColumn(None, precision, scale, nullable, None, list(blocks), ptrs, pre)
 
     @property
     def value_bytes(self) -> int:
@@ -38,14 +58,16 @@ class DeviceColumn:
     def rows(self) -> int:
         if self.indices is not None:
             return self.indices.numel()
+        if self.blocks is not None:
+            return int(self.block_prefix[-1].item())
         return self.data.numel() // self.value_bytes
 
     def up_column(self) -> abi.UpColumn:
         c = abi.UpColumn()
-        c.data = self.data.data_ptr()
-        c.blocks = None
-        c.block_prefix = None
-        c.n_blocks = 0
+        c.data = self.data.data_ptr() if self.data is not None else None
+        c.blocks = self.block_ptrs.data_ptr() if self.blocks is not None else None
+        c.block_prefix = self.block_prefix.data_ptr() if self.blocks is not None else None
+        c.n_blocks = len(self.blocks) if self.blocks is not None else 0
         c.indices = self.indices.data_ptr() if self.indices is not None else None
         c.precision = self.precision
         c.scale = self.scale
@@ -85,6 +107,10 @@ class ExprModule:
         p, s, vb = C.c_int32(), C.c_int32(), C.c_int32()
         abi.check(lib.up_module_result_type(h, C.byref(p), C.byref(s), C.byref(vb)), "up_module_result_type")
         self.precision, self.scale, self.value_bytes = p.value, s.value, vb.value
+
+    @property
+    def threads_per_value(self) -> int:
+        return int(abi.load().up_module_threads_per_value(self._h))
 
     def source(self) -> str:
         lib = abi.load()

@@ -16,7 +16,8 @@ QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
 
 class UpServeOpts(C.Structure):
     _fields_ = [("n_streams", C.c_int32), ("max_inflight", C.c_int32), ("memory_cap_bytes", C.c_int64),
-                ("reserve_bytes", C.c_int64), ("heavy_work", C.c_double)]
+                ("reserve_bytes", C.c_int64), ("heavy_work", C.c_double), ("merge", C.c_int32),
+                ("max_batch", C.c_int32), ("batch_window_us", C.c_double)]
 
 
 class UpServeRequest(C.Structure):
@@ -29,7 +30,7 @@ class UpServeStats(C.Structure):
                 ("outstanding_bytes", C.c_int64), ("max_outstanding_bytes", C.c_int64),
                 ("budget_bytes", C.c_int64), ("max_inflight_seen", C.c_int32), ("pad", C.c_int32),
                 ("p50_ms", C.c_double), ("p95_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
-                ("max_ms", C.c_double)]
+                ("max_ms", C.c_double), ("merged_launches", C.c_int64), ("merged_requests", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
@@ -53,9 +54,11 @@ def percentiles(lat_ms: Sequence[float]):
 
 class Session:
     def __init__(self, n_streams: int = 0, max_inflight: int = 0, memory_cap_bytes: int = 0,
-                 reserve_bytes: int = 0, heavy_work: float = 0.0):
+                 reserve_bytes: int = 0, heavy_work: float = 0.0, merge: bool = False, max_batch: int = 0,
+                 batch_window_us: float = 0.0):
         lib = abi.load()
-        o = UpServeOpts(n_streams, max_inflight, memory_cap_bytes, reserve_bytes, heavy_work)
+        o = UpServeOpts(n_streams, max_inflight, memory_cap_bytes, reserve_bytes, heavy_work, 1 if merge else 0,
+                        max_batch, batch_window_us)
         h = C.c_void_p()
         abi.check(lib.up_serve_create(C.byref(o), C.byref(h)), "up_serve_create")
         self._h = h

@@ -305,3 +305,37 @@ def coop_cases():
         e, types = sin_expr(p)
         out.append(("sin", p, e, types, tpv))
     return out
+
+
+# Cost-model data: launches measured on the device to train the model
+# (COSTMODEL_TRAIN) and held-out shapes it has never seen on which its choice
+# of threads per value is compared with the width rule (COSTMODEL_EVAL).
+# Columns are DECIMAL(p, p/4) with every digit uniform; rows 64K..1M.
+COSTMODEL_TRAIN_P = (40, 80, 150, 300, 600)
+COSTMODEL_EVAL_P = (60, 110, 220, 450)
+COSTMODEL_ROWS = (1 << 16, 1 << 18, 1 << 20)
+
+
+def _cm_cols(p: int, n: int):
+    return [E.ColType(p, p // 4)] * n
+
+
+def costmodel_train_shapes():
+    """(name, expression, column types) of the training launches."""
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    out = []
+    for p in COSTMODEL_TRAIN_P:
+        for name, e, n in (("mad", a * b + c, 3), ("mul", a * b, 2), ("div", a / b, 2),
+                           ("sq", (a + b) * (a - b), 2), ("mix", a * b - c * a, 3)):
+            out.append((f"{name} p={p}", e, _cm_cols(p, n)))
+    return out
+
+
+def costmodel_eval_shapes():
+    """Held-out shapes: other precisions and other expressions."""
+    a, b, c = E.col(0), E.col(1), E.col(2)
+    out = []
+    for p in COSTMODEL_EVAL_P:
+        for name, e, n in (("abc", a * b * c, 3), ("msum", a * b + c * b, 3), ("dmix", (a - b) / c + a, 3)):
+            out.append((f"{name} p={p}", e, _cm_cols(p, n)))
+    return out
