@@ -1,31 +1,44 @@
 """Benchmark of the exact-decimal path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sweep|batch|query|sin|serve|text]
+                    [--workload all|sweep|batch|query|sin|serve|text|filter]
 
-Workload "sweep" (default) is the precision sweep: element-wise a*b+c and a/b
-(scale s+4, half-up) on DECIMAL(p, p/4), p in {18,38,76,150,300,600}, every
-digit uniform 0-9, signs +/-, zero divisors redrawn, 16M rows for p<=38,
-halved per doubling of p.  One step = one pass over all twelve
-(p, expression) launches; inputs are resident in HBM and every case's input
-is larger than L2 (126 MB), so no L2 flush is needed between steps.
+The default workload "all" prints one JSON line whose headline record is the
+precision sweep, with the other workload definitions as sub-records under
+"configs" (each with its own roofline, e2e, output check and CPU baseline):
 
-Workload "batch" is the batched mixed-precision set: 64 seeded tasks (random
-+,-,*,/ trees of depth 3-5 on 2-4 DECIMAL(p,s) columns, p log-uniform in
-[10,400], rows log-uniform in [1e3,1e7], half ending in a grouped SUM over
-Zipf(1.1) keys) run as one captured graph of persistent band kernels, beside
-the same 64 tasks launched one by one through the plain per-task path.  A
-step is one pass over all 64 tasks; inputs total about 7.5 GB, larger than L2.
+* sweep (headline): element-wise a*b+c and a/b (scale s+4, half-up) on
+  DECIMAL(p, p/4), p in {18,38,76,150,300,600}, every digit uniform 0-9, signs
+  +/-, zero divisors redrawn, 16M rows for p<=38, halved per doubling of p.
+  One step = one pass over all twelve (p, expression) launches; inputs are
+  resident in HBM and every case's input is larger than L2 (126 MB), so no L2
+  flush is needed between steps.
+* 0_grouped_query: SUM x4 / AVG x3 / COUNT over four DECIMAL(15,2) columns
+  grouped by two CHAR(1) keys, at 1M and 256M rows.
+* 2_batch: 64 seeded tasks (random +,-,*,/ trees of depth 3-5 on 2-4
+  DECIMAL(p,s) columns, p log-uniform in [10,400], rows log-uniform in
+  [1e3,1e7], half ending in a grouped SUM over Zipf(1.1) keys) run as one
+  captured graph of persistent band kernels, beside the same 64 tasks launched
+  one by one through the plain per-task path.
+* 3_sin: sin(x) by a 20-term Horner series on DECIMAL(p, p-2), p=100/300/1000.
+* 4_serve: open-loop Poisson arrivals at 100/500/2000/5000 queries/s over
+  resident columns (2 s of arrivals per rate by default, --serve-seconds).
+
+Every record checks its GPU outputs against the oracle on the same input bytes
+(sampled row ranges, or whole small cases) and exits non-zero on a mismatch.
 
 The reference arm (--impl reference) times the CPU restatement of the
-reference's decimal path (oracle/, the reference has no CPU decimal path of
-its own) on the host cores, on a bounded sample of the same workload.
+reference's decimal path (oracle/; the reference has no CPU decimal path of
+its own) on all host cores: every step is a bounded sample of the same
+workload, its ms_per_step is the measured time of that sample, and its config
+is the one our arm reports.  It loads no library of the product.
 """
 from __future__ import annotations
 
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import subprocess
 import sys
@@ -45,9 +58,19 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "query", "sin", "serve", "text", "filter"])
-    ap.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per rate (serve workload)")
+    ap.add_argument("--workload", default="all",
+                    choices=["all", "sweep", "batch", "query", "sin", "serve", "text", "filter", "costmodel"],
+                    help="all (default): the precision sweep as the headline record, the grouped query, the "
+                         "batched set, the sin series and the served stream as sub-records under 'configs'")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="arrival window per rate (serve workload); the workload definition asks 300")
+    ap.add_argument("--serve-window-us", type=float, default=250.0,
+                    help="batching window of the merged-launch session (serve workload)")
+    ap.add_argument("--serve-heavy", action="store_true", help="also run the low-priority heavy-request session")
+    ap.add_argument("--serve-out", default="", help="write the full per-rate serve table to this JSON file")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--ref-seconds", type=float, default=90.0,
+                    help="reference arm: target CPU time of all its steps (warm-up included), every record")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only", default="", help="comma list of p:op sweep cases (profiling a subset)")
@@ -118,22 +141,26 @@ def limbs(nbytes: int) -> int:
     return (nbytes + 3) // 4
 
 
-def sweep_cases(scale_rows: float = 1.0):
-    from ultraprecise_b200 import codec
+def sweep_cases(scale_rows: float = 1.0, compact_bytes=None):
+    """The twelve sweep cases with their algorithmic bytes and limb work per
+    row.  compact_bytes: the byte table to use (the library's by default; the
+    reference arm passes the oracle's so that it never loads the library)."""
+    if compact_bytes is None:
+        from ultraprecise_b200.codec import compact_bytes
     cases = []
     for p, rows in SWEEP:
         s = p // 4
-        B = codec.compact_bytes(p)
+        B = compact_bytes(p)
         for op in ("mad", "div"):
             r = max(1, int(rows * scale_rows))
             if op == "mad":
-                ob = codec.compact_bytes(2 * p + 1)
+                ob = compact_bytes(2 * p + 1)
                 nin = 3
                 # limb multiply-adds per row: the a*b product plus aligning c by 10^s
                 la = limbs(B)
                 madds = la * la + la * limbs(max(1, ((10 ** s).bit_length() + 7) // 8))
             else:
-                ob = codec.compact_bytes(max(s + 5, 1))
+                ob = compact_bytes(max(s + 5, 1))
                 nin = 2
                 sh = s + 4
                 la = limbs(B)
@@ -248,19 +275,60 @@ def run_ours(args, rank, world):
     res = {"metric": METRIC, "value": round(value), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-           "config": {"workload": "precision sweep: a*b+c and a/b on DECIMAL(p,p/4), "
-                                  "p in 18,38,76,150,300,600; 16M rows p<=38 halved per doubling",
-                      "rows_per_step_per_gpu": rows_per_step, "l2": "inputs larger than L2 (no flush)",
-                      "parallelism": f"replicas x{world} (row shards, no collective)"},
+           "config": sweep_config(world, rows_per_step),
            "roofline": roof, "cases": case_rep,
            "gpu_launches": len(cases) * args.steps,
            "imad_peak_gmadds": round(madd_peak.value / 1e9, 1)}
     res["clocks"] = clk.summary()
+    res["imad_theoretical"] = imad_theoretical(madd_peak.value, res["clocks"])
     if not args.no_e2e:
         res["e2e"] = e2e_ours(args, cases, mods, world, stream)
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
-        res["cpu_baseline"] = cpu_baseline(cases, args.cpu_seconds)
+    if not args.no_cpu_baseline:
+        # the CPU leg: every case's output checked on sampled row ranges
+        # against the oracle (all ranks), then the oracle timed (rank 0, N=1)
+        torch.cuda.synchronize()
+        res["verified"] = verify_sweep(cases, mods, inputs, outs)
+        if not res["verified"]["ok"]:
+            raise SystemExit("sweep outputs differ from the oracle: " + json.dumps(res["verified"]))
+        if rank == 0 and world == 1:
+            res["cpu_baseline"] = cpu_sweep(cases, args.cpu_seconds)
     return res
+
+
+def sweep_config(world, rows_per_step):
+    """The sweep's config object, identical in both arms."""
+    return {"workload": "precision sweep: a*b+c and a/b on DECIMAL(p,p/4), "
+                        "p in 18,38,76,150,300,600; 16M rows p<=38 halved per doubling",
+            "rows_per_step_per_gpu": rows_per_step, "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas x{world} (row shards, no collective)"}
+
+
+def imad_theoretical(measured, clocks):
+    """The integer pipe's theoretical limb multiply-add rate at the SM clock
+    seen under load and at the maximum clock, and the measured probe peak as
+    a fraction of it.  Basis: 64 32-bit integer multiply-adds per clock per
+    SM (the throughput of 32-bit multiply / multiply-add for compute
+    capability 7.0 and later), two of them per limb multiply-add (the low and
+    the high half of the 64-bit product): 32 limb multiply-adds per clock per
+    SM."""
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    except Exception:
+        sms = 148
+    per_clk = sms * 32
+    out = {"limb_madds_per_clk_per_sm": 32, "sms": sms}
+    for key, mhz in (("at_load_clock", clocks.get("sm_mhz")), ("at_max_clock", clocks.get("sm_max_mhz"))):
+        if mhz:
+            g = per_clk * mhz * 1e6 / 1e9
+            out[key] = {"mhz": mhz, "gmadds": round(g, 1), "measured_frac": round(measured / 1e9 / g, 4)}
+    return out
+
+
+def e2e_steps(args):
+    """Timed steps of an end-to-end figure: as many as the device figure,
+    bounded to 10 (a step moves every input and result over the host link)."""
+    return max(3, min(args.steps, 10))
 
 
 def e2e_ours(args, cases, mods, world, stream):
@@ -289,8 +357,8 @@ def e2e_ours(args, cases, mods, world, stream):
         for i, (c, m) in enumerate(zip(cases, mods)):
             m.launch_host(host_in[i], [E.ColType(c["p"], c["s"])] * c["n_in"], c["rows"], host_out[i])
 
-    steps = max(1, min(args.steps, 3))
-    for _ in range(max(1, min(args.warmup, 2))):
+    steps = e2e_steps(args)
+    for _ in range(max(2, min(args.warmup, 3))):
         step()
     torch.cuda.synchronize()
     barrier(world)
@@ -425,10 +493,7 @@ def run_batch(args, rank, world):
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_batch, 4),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-           "config": {"workload": "64-task batched mixed precision (seeded trees, p 10-400, rows 1e3-1e7, half "
-                                  "grouped SUM over Zipf(1.1) keys)", "rows_per_step_per_gpu": rows,
-                      "tree_redraws": redraws, "l2": "inputs larger than L2 (no flush)",
-                      "parallelism": f"replicas x{world} (no collective)"},
+           "config": batch_config(world, rows, redraws),
            "rows_per_s": round(rows * world / (ms_batch * 1e-3)),
            "plain": {"ms_per_step": round(ms_plain, 4), "queries_per_s": round(n * world / (ms_plain * 1e-3), 2),
                      "speedup_batched": round(ms_plain / ms_batch, 3), "byte_equal": same},
@@ -445,9 +510,45 @@ def run_batch(args, rank, world):
                b.task_type(k)[3] == i for k in range(n)))), "clocks": clocks}
     if not args.no_e2e:
         res["e2e"] = e2e_batch(args, b, tasks, data, outs, gids, world, stream)
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
-        res["cpu_baseline"] = cpu_baseline_batch(tasks, args.cpu_seconds)
+    if not args.no_cpu_baseline:
+        res["verified"] = verify_batch(tasks, data, outs)
+        if not res["verified"]["ok"] or not same:
+            raise SystemExit("batch outputs differ: " + json.dumps(res["verified"]) + f" plain_equal={same}")
+        if rank == 0 and world == 1:
+            res["cpu_baseline"] = cpu_batch(tasks, args.cpu_seconds)
     return res
+
+
+def batch_config(world, rows, redraws):
+    return {"workload": "64-task batched mixed precision (seeded trees, p 10-400, rows 1e3-1e7, half "
+                        "grouped SUM over Zipf(1.1) keys)", "rows_per_step_per_gpu": rows,
+            "tree_redraws": redraws, "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas x{world} (no collective)"}
+
+
+def verify_batch(tasks, data, outs, max_rows=20000):
+    """Every task of at most max_rows rows recomputed by the oracle from the
+    same input bytes (projections byte for byte, grouped SUMs image for image);
+    the larger tasks are covered by the byte equality with the plain per-task
+    launches."""
+    orc = _oracle()
+    bad, checked, n = [], 0, 0
+    for k, (t, (rows, cols, gid), o) in enumerate(zip(tasks, data, outs)):
+        if rows > max_rows:
+            continue
+        b = _built([t["expr"]], t["cols"])
+        host = [_host(c, 0, c.numel()) for c in cols]
+        if t["agg"] < 0:
+            ob = orc.compact_bytes(b.nodes[b.roots[0]].precision)
+            exp, _ = orc.eval_expr(b, b.roots[0], host, rows, ob)
+        else:
+            exp = orc.query(b, [(t["agg"], b.roots[0])], host, gid.tobytes(), rows, t["groups"])[0]
+        n += 1
+        checked += rows
+        if _host(o, 0, len(exp)) != exp:
+            bad.append(f"task {k}")
+    return {"ok": not bad, "tasks_checked": n, "rows_checked": checked, "mismatches": bad,
+            "how": f"tasks of <= {max_rows} rows vs the oracle; all tasks vs the plain per-task launches"}
 
 
 def e2e_batch(args, b, tasks, data, outs, gids, world, stream):
@@ -477,8 +578,9 @@ def e2e_batch(args, b, tasks, data, outs, gids, world, stream):
             for h, d in pairs_out:
                 h.copy_(d, non_blocking=True)
 
-    steps = max(1, min(args.steps, 3))
-    step()
+    steps = e2e_steps(args)
+    for _ in range(2):
+        step()
     torch.cuda.synchronize()
     barrier(world)
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -490,49 +592,6 @@ def e2e_batch(args, b, tasks, data, outs, gids, world, stream):
     ms = max_over_ranks(t0.elapsed_time(t1), world) / steps
     return {"value": round(len(tasks) * world / (ms * 1e-3), 2), "unit": "queries/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": steps}
-
-
-def batch_cpu_rate(tasks, cpu_seconds, threads, seed=1):
-    """Oracle time for the 64 tasks on the host cores, every task at one common
-    fraction of its rows, extrapolated to full rows: (queries/s, fraction, rows)."""
-    import numpy as np
-    from oracle import gen, oracle
-    from ultraprecise_b200 import codec, workloads
-    from ultraprecise_b200 import expr as E
-
-    def run(frac):
-        secs, rows_tot = 0.0, 0
-        for k, t in enumerate(tasks):
-            r = max(4, int(t["rows"] * frac))
-            nb = codec.compact_bytes(t["p"])
-            cols = [gen.compact_digits(r, t["p"], nb, seed + 97 * k + c, nonzero=True) for c in range(t["ncols"])]
-            bt = E.build([t["expr"]], t["cols"])
-            E.derive_types(bt)
-            if t["agg"] < 0:
-                ob = codec.compact_bytes(bt.nodes[bt.roots[0]].precision)
-                t0 = time.perf_counter()
-                oracle.eval_expr(bt, bt.roots[0], cols, r, ob, threads=threads)
-            else:
-                g = workloads.batch_group_ids(r, t["groups"], seed + k).tobytes()
-                t0 = time.perf_counter()
-                oracle.query(bt, [(t["agg"], bt.roots[0])], cols, g, r, t["groups"], threads=threads)
-            secs += time.perf_counter() - t0
-            rows_tot += r
-        return secs, rows_tot
-
-    f0 = 1.0 / 4096
-    s0, _ = run(f0)
-    frac = min(1.0 / 8, f0 * cpu_seconds / max(s0, 1e-4))
-    s1, rows = run(frac)
-    return len(tasks) / (s1 / frac), frac, rows
-
-
-def cpu_baseline_batch(tasks, cpu_seconds):
-    threads = os.cpu_count() or 1
-    rate, frac, rows = batch_cpu_rate(tasks, cpu_seconds, threads)
-    return {"value": round(rate, 4), "unit": "queries/s", "cores": threads, "kind": "port",
-            "sample": f"{rows} rows: every task at {frac:.2e} of its rows, time scaled to full rows; oracle on "
-                      f"{threads} host threads"}
 
 
 # ------------------------------------------------------------ query workload
@@ -574,7 +633,7 @@ def run_query(args, rank, world):
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     table = torch.empty(abi.UP_KEY_TABLE_ENTRIES, dtype=torch.int32, device="cuda")
     keyb = [1, 1]
-    results = {}
+    results, checks = {}, {}
 
     def timed(fn, n):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -634,6 +693,10 @@ def run_query(args, rank, world):
                           "hbm_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
                           "two_pass_group_ids_ms": round(ids_ms, 4), "graph_replay_ms": round(graph_ms, 4),
                           "clocks": clk.summary()}
+        if not args.no_cpu_baseline:  # the CPU leg checks the outputs of this size
+            torch.cuda.synchronize()
+            checks[label] = (verify_query_full(q, aggs, cols, k1, k2, outs, G) if label == "1M"
+                             else verify_query_sums(cols, k1, k2, outs, aggs, G))
         if label == "256M":
             main = results[label]
             inputs = (cols, k1, k2, table, G, outs)
@@ -643,10 +706,7 @@ def run_query(args, rank, world):
     res = {"metric": QUERY_METRIC, "value": m["rows_per_s"], "unit": "rows/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-           "config": {"workload": f"grouped SUMx4/AVGx3/COUNT query, DECIMAL(15,2) x4, 2 CHAR(1) keys, "
-                                  f"{m['rows']} rows, step = key table + fused query, no host round trip "
-                                  f"(256M roofline run; 1M-row case in 'rows_1m')",
-                      "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world} (no collective)"},
+           "config": query_config(world, m["rows"]),
            "roofline": {"bound": "hbm", "achieved": m["hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
                         "frac": m["hbm_frac"], "traffic": None, "kernel": "up_query_tile_r (+ up_query_fin)",
                         "peak_source": peak_kind, "bytes_per_row": QUERY_BYTES_PER_ROW},
@@ -654,12 +714,20 @@ def run_query(args, rank, world):
            "rows_1m": results["1M"], "gpu_launches": 5 * args.steps, "clocks": m["clocks"]}
     if not args.no_e2e:
         res["e2e"] = e2e_query(args, q, aggs, inputs, world, stream)
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
-        rate, rows = query_cpu_rate(args.cpu_seconds, os.cpu_count() or 1)
-        res["cpu_baseline"] = {"value": round(rate), "unit": "rows/s", "cores": os.cpu_count() or 1,
-                               "kind": "port", "sample": f"{rows} rows of the same query (group ids given), "
-                                                         f"oracle on {os.cpu_count() or 1} host threads"}
+    if not args.no_cpu_baseline:
+        res["verified"] = {"rows_1m": checks.get("1M"), "rows_256m": checks.get("256M")}
+        if not all(v and v["ok"] for v in res["verified"].values()):
+            raise SystemExit("grouped query outputs differ: " + json.dumps(res["verified"]))
+        if rank == 0 and world == 1:
+            res["cpu_baseline"] = cpu_query(args.cpu_seconds)
     return res
+
+
+def query_config(world, rows):
+    return {"workload": f"grouped SUMx4/AVGx3/COUNT query, DECIMAL(15,2) x4, 2 CHAR(1) keys, "
+                        f"{rows} rows, step = key table + fused query, no host round trip "
+                        f"(256M roofline run; 1M-row case in 'rows_1m')",
+            "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world} (no collective)"}
 
 
 def e2e_query(args, q, aggs, inputs, world, stream):
@@ -689,10 +757,11 @@ def e2e_query(args, q, aggs, inputs, world, stream):
             for h, o in zip(hout, outs):
                 h.copy_(o, non_blocking=True)
 
-    step()
+    for _ in range(2):
+        step()
     torch.cuda.synchronize()
     barrier(world)
-    steps = max(1, min(args.steps, 3))
+    steps = e2e_steps(args)
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     for _ in range(steps):
@@ -703,37 +772,6 @@ def e2e_query(args, q, aggs, inputs, world, stream):
     rows = k1.numel()
     return {"value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": round(ms, 3), "steps": steps}
-
-
-def query_cpu_rate(cpu_seconds, threads, seed=3):
-    """Oracle rows/s for the query on the host cores, sized for ~cpu_seconds."""
-    import numpy as np
-    from oracle import gen, oracle
-    from ultraprecise_b200 import workloads
-    from ultraprecise_b200 import expr as E
-    exprs, aggs, ctypes_ = workloads.query_exprs()
-    b = E.build(exprs, ctypes_)
-    E.derive_types(b)
-    qa = [(k, b.roots[i]) for k, i in aggs]
-
-    def run(rows):
-        rng = np.random.default_rng(seed)
-        R = workloads.QUERY_RANGES
-        cols = []
-        for n in ("qty", "price", "disc", "tax"):
-            lo, hi, st = R[n]
-            v = lo + st * rng.integers(0, (hi - lo) // st + 1, rows, dtype=np.int64)
-            cols.append(gen.pack_unsigned(v, 7))
-        w = np.array([k[2] for k in workloads.QUERY_KEYS])
-        g = rng.choice(len(w), size=rows, p=w / w.sum()).astype(np.int32).tobytes()
-        t = time.perf_counter()
-        oracle.query(b, qa, cols, g, rows, len(w), threads=threads)
-        return time.perf_counter() - t
-
-    r0 = 1 << 16
-    s0 = run(r0)
-    rows = int(min(1 << 28, r0 * cpu_seconds / max(s0, 1e-4)))
-    return rows / run(rows), rows
 
 
 # ------------------------------------------------------------ sin workload
@@ -808,9 +846,7 @@ def run_sin(args, rank, world):
     res = {"metric": SIN_METRIC, "value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-           "config": {"workload": "sin(x) 20-term Horner on DECIMAL(p,p-2): 1M rows p=100, 512K p=300, "
-                                  "256K p=1000; x uniform in [-pi, pi]", "rows_per_step_per_gpu": rows,
-                      "l2": "compute-bound; inputs stay resident", "parallelism": f"replicas x{world}"},
+           "config": sin_config(world, rows),
            "roofline": {"bound": "int32", "achieved": rep[dom]["int_gmadds"],
                         "peak": round(madd_peak.value / 1e9, 1), "unit": "G limb-madd/s",
                         "frac": rep[dom]["int_frac"], "traffic": None,
@@ -830,9 +866,10 @@ def run_sin(args, rank, world):
                     launch(c)
                     ho.copy_(c["out"], non_blocking=True)
 
-        e2e_step()
+        for _ in range(2):
+            e2e_step()
         torch.cuda.synchronize()
-        n = max(1, min(args.steps, 3))
+        n = e2e_steps(args)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(n):
@@ -842,41 +879,25 @@ def run_sin(args, rank, world):
         ems = max_over_ranks(e0.elapsed_time(e1), world) / n
         res["e2e"] = {"value": round(rows * world / (ems * 1e-3)), "unit": "rows/s", "h2d_bytes_per_step": h2d,
                       "d2h_bytes_per_step": d2h, "ms_per_step": round(ems, 3), "steps": n}
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
-        rate, sample = sin_cpu_rate(args.cpu_seconds, os.cpu_count() or 1)
-        res["cpu_baseline"] = {"value": round(rate), "unit": "rows/s", "cores": os.cpu_count() or 1, "kind": "port",
-                               "sample": sample}
+    if not args.no_cpu_baseline:
+        bad, checked = [], 0
+        for c in cases:
+            b, n = verify_rows(c["mod"], [c["in"]], c["out"], c["rows"], slice_rows=32)
+            bad += [f"p={c['p']} {x}" for x in b]
+            checked += n
+        res["verified"] = {"ok": not bad, "rows_checked": checked, "mismatches": bad,
+                           "how": "3 row ranges of 32 per case vs the oracle on the same input bytes"}
+        if bad:
+            raise SystemExit("sin outputs differ from the oracle: " + json.dumps(res["verified"]))
+        if rank == 0 and world == 1:
+            res["cpu_baseline"] = cpu_sin(args.cpu_seconds)
     return res
 
 
-def sin_cpu_rate(cpu_seconds, threads, seed=11):
-    """Oracle rows/s over the same three-precision mix, every case at one
-    common fraction of its rows, sized for ~cpu_seconds."""
-    from oracle import oracle
-    from ultraprecise_b200 import codec, workloads
-    from ultraprecise_b200 import expr as E
-    built = []
-    for p, rows in workloads.SIN:
-        e, cols = workloads.sin_expr(p)
-        b = E.build([e], cols)
-        E.derive_types(b)
-        built.append((p, rows, b))
-
-    def run(frac):
-        secs, tot = 0.0, 0
-        for p, rows, b in built:
-            r = max(8, int(rows * frac))
-            raw = workloads.sin_inputs(p, r, seed + p)
-            t = time.perf_counter()
-            oracle.eval_expr(b, b.roots[0], [raw], r, codec.compact_bytes(p), threads=threads)
-            secs += time.perf_counter() - t
-            tot += r
-        return tot, secs
-
-    r0, s0 = run(1.0 / 2048)
-    frac = min(1.0 / 8, (1.0 / 2048) * cpu_seconds / max(s0, 1e-4))
-    r1, s1 = run(frac)
-    return r1 / s1, f"{r1} rows: every case at {frac:.2e} of its rows (same mix), oracle on {threads} host threads"
+def sin_config(world, rows):
+    return {"workload": "sin(x) 20-term Horner on DECIMAL(p,p-2): 1M rows p=100, 512K p=300, "
+                        "256K p=1000; x uniform in [-pi, pi]", "rows_per_step_per_gpu": rows,
+            "l2": "compute-bound; inputs stay resident", "parallelism": f"replicas x{world}"}
 
 
 # ------------------------------------------------------------ serve workload
@@ -947,8 +968,8 @@ def run_serve(args, rank, world):
         rng = random.Random(int(rate) * 13 + rank)
         return [(t, kinds[k][rng.randrange(len(kinds[k]))]) for t, k in zip(arr, kk)]
 
-    def run_session(tr, heavy_work=0.0):
-        sess = serve.Session(n_streams=8, heavy_work=heavy_work)
+    def run_session(tr, heavy_work=0.0, merge=False, window_us=0.0):
+        sess = serve.Session(n_streams=8, heavy_work=heavy_work, merge=merge, batch_window_us=window_us)
         t0 = sess.clock_ms()
         pending = collections.deque()
         lat, mismatches, checked = [], 0, 0
@@ -987,6 +1008,7 @@ def run_serve(args, rank, world):
         return {"queries": len(tr), "seconds": round(end / 1e3, 3), "queries_per_s": round(len(tr) / (end / 1e3), 1),
                 "p50_ms": round(p50, 3), "p95_ms": round(p95, 3), "p99_ms": round(p99, 3),
                 "max_inflight": st["max_inflight_seen"], "deferred": st["deferred"],
+                "merged_launches": st["merged_launches"], "merged_requests": st["merged_requests"],
                 "max_outstanding_gb": round(st["max_outstanding_bytes"] / 1e9, 3),
                 "sampled_byte_equal": mismatches == 0, "sampled": checked}
 
@@ -1012,14 +1034,22 @@ def run_serve(args, rank, world):
 
     warm = trace(200.0)[:50]
     run_session(warm)
+    run_session(warm, merge=True, window_us=args.serve_window_us)
     run_plain(warm)
     rates = {}
     with ClockSampler(dev) as clk:
         for rate in workloads.SERVE_RATES:
             tr = trace(float(rate))
-            rates[str(rate)] = {"served": run_session(tr), "served_heavy_lowprio": run_session(tr, 1e9),
+            rates[str(rate)] = {"served": run_session(tr),
+                                "served_merged": run_session(tr, merge=True, window_us=args.serve_window_us),
                                 "plain": run_plain(tr)}
+            if args.serve_heavy:
+                rates[str(rate)]["served_heavy_lowprio"] = run_session(tr, 1e9)
     top = rates[str(workloads.SERVE_RATES[-1])]
+    if args.serve_out:
+        with open(args.serve_out, "w") as f:
+            json.dump({"serve_seconds": args.serve_seconds, "window_us": args.serve_window_us, "rates": rates}, f,
+                      indent=1)
     # value: the highest offered rate's served throughput
     res = {"metric": SERVE_METRIC, "value": top["served"]["queries_per_s"], "unit": "queries/s", "n_gpus": world,
            "steps": len(workloads.SERVE_RATES), "warmup": 1, "ms_per_step": round(top["served"]["seconds"] * 1e3, 1),
@@ -1091,28 +1121,6 @@ def run_text(args, rank, world):
 FILTER_METRIC = "decimal rows/s filtered (WHERE a*b >= c AND a <> 0 over DECIMAL(38,9), kept row indices), bit-exact"
 
 
-def filter_cpu_rate(cpu_seconds, threads, seed=9):
-    """Oracle rows/s for the predicate plus numpy's nonzero on the host."""
-    import numpy as np
-    from oracle import gen, oracle
-    from ultraprecise_b200 import expr as E
-    e, ct = filter_expr()
-    b = E.build([e], ct)
-    E.derive_types(b)
-
-    def run(rows):
-        cols = [gen.compact_digits(rows, 38, 16, seed + k) for k in range(3)]
-        t = time.perf_counter()
-        flags, _ = oracle.eval_expr(b, b.roots[0], cols, rows, 1, threads=threads)
-        np.nonzero(np.frombuffer(flags, dtype=np.uint8))
-        return time.perf_counter() - t
-
-    r0 = 1 << 14
-    s0 = run(r0)
-    rows = int(min(1 << 26, r0 * cpu_seconds / max(s0, 1e-4)))
-    return rows / run(rows), rows
-
-
 def filter_expr():
     from ultraprecise_b200 import expr as E
     a, b, c = E.col(0), E.col(1), E.col(2)
@@ -1177,9 +1185,7 @@ def run_filter(args, rank, world):
     res = {"metric": FILTER_METRIC, "value": round(rows * world / (ms * 1e-3)), "unit": "rows/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-           "config": {"workload": f"predicate + row selection over {rows} rows of 3 DECIMAL(38,9) columns, "
-                                  f"{kept} rows kept", "l2": "inputs larger than L2 (no flush)",
-                      "parallelism": f"replicas x{world} (no collective)"},
+           "config": filter_config(world, rows), "rows_kept": kept,
            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
                         "frac": round(gbs / hbm_peak, 4), "traffic": None, "kernel": "up_expr_tile (predicate)",
                         "peak_source": peak_kind, "bytes_per_row": pred_bytes},
@@ -1201,148 +1207,504 @@ def run_filter(args, rank, world):
             with torch.cuda.stream(stream):
                 hidx[:kept].copy_(idx[:kept], non_blocking=True)
 
-        e2e_step()
+        for _ in range(2):
+            e2e_step()
         torch.cuda.synchronize()
-        n = max(1, min(args.steps, 3))
+        n = e2e_steps(args)
         ems = max_over_ranks(timed(e2e_step, n), world)
         res["e2e"] = {"value": round(rows * world / (ems * 1e-3)), "unit": "rows/s",
                       "h2d_bytes_per_step": 3 * 16 * rows, "d2h_bytes_per_step": 4 * kept,
                       "ms_per_step": round(ems, 3), "steps": n}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        rate, srows = filter_cpu_rate(args.cpu_seconds, os.cpu_count() or 1)
-        res["cpu_baseline"] = {"value": round(rate), "unit": "rows/s", "cores": os.cpu_count() or 1, "kind": "port",
-                               "sample": f"{srows} rows of the same predicate and selection, oracle on "
-                                         f"{os.cpu_count() or 1} host threads"}
+        res["cpu_baseline"] = cpu_filter(args.cpu_seconds)
     return res
 
 
-# ------------------------------------------------------ CPU baseline
-def cpu_rate(cases, cpu_seconds, threads, seed=1):
-    """Time the oracle on the host cores over the same sweep mix (every case
-    scaled by one common fraction of its rows), sized for ~cpu_seconds."""
-    from oracle import gen, oracle
-    from ultraprecise_b200 import codec
-    from ultraprecise_b200 import expr as E
+def filter_config(world, rows):
+    return {"workload": f"predicate + row selection over {rows} rows of 3 DECIMAL(38,9) columns",
+            "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world} (no collective)"}
 
-    def run(frac):
-        rows_tot, secs = 0, 0.0
+
+# ------------------------------------------------------ CPU leg (oracle)
+# The oracle (oracle/: a CPU restatement of the reference's decimal path,
+# whose own arithmetic is device-only) has two roles here and no other: it is
+# timed on the host cores (the CPU baseline of our arm, and the reference
+# arm), and it checks sampled outputs of the GPU runs.  Its inputs are
+# prepared before the timed region, typed by the oracle's own typing
+# restatement and sized with its own byte table, so the reference arm never
+# loads the product library.
+def _oracle():
+    from oracle import oracle
+    return oracle
+
+
+def _built(exprs, ctypes_):
+    from ultraprecise_b200 import expr as E
+    b = E.build(list(exprs), ctypes_)
+    _oracle().derive_types(b)
+    return b
+
+
+class SweepRunner:
+    """Every sweep case at one common fraction of its rows."""
+
+    def __init__(self, cases, frac, threads, seed=1):
+        from oracle import gen
+        orc = _oracle()
+        self.threads, self.items, self.rows = threads, [], 0
         for i, c in enumerate(cases):
             r = max(8, int(c["rows"] * frac))
             cols = [gen.compact_digits(r, c["p"], c["in_bytes"], seed + 31 * i + k,
                                        nonzero=(c["op"] == "div" and k == 1)) for k in range(c["n_in"])]
             e, ct = build_expr(c)
-            b = E.build([e], ct)
-            E.derive_types(b)
-            ob = codec.compact_bytes(b.nodes[b.roots[0]].precision)
-            t = time.perf_counter()
-            oracle.eval_expr(b, b.roots[0], cols, r, ob, threads=threads)
-            secs += time.perf_counter() - t
-            rows_tot += r
-        return rows_tot, secs
+            b = _built([e], ct)
+            self.items.append((b, cols, r, orc.compact_bytes(b.nodes[b.roots[0]].precision)))
+            self.rows += r
 
-    f0 = 1.0 / 65536
-    r0, s0 = run(f0)
-    frac = min(1.0 / 16, f0 * cpu_seconds / max(s0, 1e-4))
-    r1, s1 = run(frac)
-    return r1 / s1, frac, r1
+    def step(self):
+        orc = _oracle()
+        t = time.perf_counter()
+        for b, cols, r, ob in self.items:
+            orc.eval_expr(b, b.roots[0], cols, r, ob, threads=self.threads)
+        return time.perf_counter() - t
 
 
-def cpu_baseline(cases, cpu_seconds):
-    threads = os.cpu_count() or 1
-    rate, frac, rows = cpu_rate(cases, cpu_seconds, threads)
-    return {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
-            "sample": f"{rows} rows: every sweep case at {frac:.2e} of its rows (same mix), oracle on "
-                      f"{threads} host threads"}
+class QueryRunner:
+    """The grouped query (group ids given) over `rows` rows."""
+
+    def __init__(self, rows, threads, seed=3):
+        import numpy as np
+        from oracle import gen
+        from ultraprecise_b200 import workloads
+        exprs, aggs, ct = workloads.query_exprs()
+        self.b = _built(exprs, ct)
+        self.qa = [(k, self.b.roots[i]) for k, i in aggs]
+        rng = np.random.default_rng(seed)
+        R = workloads.QUERY_RANGES
+        self.cols = []
+        for n in ("qty", "price", "disc", "tax"):
+            lo, hi, st = R[n]
+            self.cols.append(gen.pack_unsigned(lo + st * rng.integers(0, (hi - lo) // st + 1, rows, dtype=np.int64), 7))
+        w = np.array([k[2] for k in workloads.QUERY_KEYS])
+        self.G = len(w)
+        self.gids = rng.choice(len(w), size=rows, p=w / w.sum()).astype(np.int32).tobytes()
+        self.rows, self.threads = rows, threads
+
+    def step(self):
+        t = time.perf_counter()
+        _oracle().query(self.b, self.qa, self.cols, self.gids, self.rows, self.G, threads=self.threads)
+        return time.perf_counter() - t
+
+
+class BatchRunner:
+    """The 64 batch tasks, every task at one common fraction of its rows."""
+
+    def __init__(self, tasks, frac, threads, seed=1):
+        from oracle import gen
+        from ultraprecise_b200 import workloads
+        orc = _oracle()
+        self.threads, self.items, self.rows, self.frac = threads, [], 0, frac
+        for k, t in enumerate(tasks):
+            r = max(4, int(t["rows"] * frac))
+            nb = orc.compact_bytes(t["p"])
+            cols = [gen.compact_digits(r, t["p"], nb, seed + 97 * k + c, nonzero=True) for c in range(t["ncols"])]
+            b = _built([t["expr"]], t["cols"])
+            g = workloads.batch_group_ids(r, t["groups"], seed + k).tobytes() if t["agg"] >= 0 else None
+            ob = orc.compact_bytes(b.nodes[b.roots[0]].precision)
+            self.items.append((t, b, cols, r, g, ob))
+            self.rows += r
+
+    def step(self):
+        orc = _oracle()
+        t0 = time.perf_counter()
+        for t, b, cols, r, g, ob in self.items:
+            if g is None:
+                orc.eval_expr(b, b.roots[0], cols, r, ob, threads=self.threads)
+            else:
+                orc.query(b, [(t["agg"], b.roots[0])], cols, g, r, t["groups"], threads=self.threads)
+        return time.perf_counter() - t0
+
+
+class SinRunner:
+    """The three sin cases at one common fraction of their rows."""
+
+    def __init__(self, frac, threads, seed=11):
+        from ultraprecise_b200 import workloads
+        orc = _oracle()
+        self.threads, self.items, self.rows = threads, [], 0
+        for p, rows in workloads.SIN:
+            e, ct = workloads.sin_expr(p)
+            r = max(8, int(rows * frac))
+            self.items.append((_built([e], ct), workloads.sin_inputs(p, r, seed + p), r, orc.compact_bytes(p)))
+            self.rows += r
+
+    def step(self):
+        orc = _oracle()
+        t = time.perf_counter()
+        for b, raw, r, ob in self.items:
+            orc.eval_expr(b, b.roots[0], [raw], r, ob, threads=self.threads)
+        return time.perf_counter() - t
+
+
+class FilterRunner:
+    """The filter predicate plus the row selection (numpy) over `rows` rows."""
+
+    def __init__(self, rows, threads, seed=9):
+        from oracle import gen
+        e, ct = filter_expr()
+        self.b = _built([e], ct)
+        self.cols = [gen.compact_digits(rows, 38, 16, seed + k) for k in range(3)]
+        self.rows, self.threads = rows, threads
+
+    def step(self):
+        import numpy as np
+        t = time.perf_counter()
+        flags, _ = _oracle().eval_expr(self.b, self.b.roots[0], self.cols, self.rows, 1, threads=self.threads)
+        np.nonzero(np.frombuffer(flags, dtype=np.uint8))
+        return time.perf_counter() - t
+
+
+def calibrate(make, target_s, x0, xmax):
+    """A runner sized so that one step takes about target_s: one trial step at
+    size x0, then the size scaled linearly (capped at xmax)."""
+    s0 = make(x0).step()
+    x = min(xmax, x0 * target_s / max(s0, 1e-4))
+    return make(x), x
+
+
+def threads_all():
+    return os.cpu_count() or 1
+
+
+def cpu_sweep(cases, cpu_seconds):
+    th = threads_all()
+    r, frac = calibrate(lambda f: SweepRunner(cases, f, th), cpu_seconds, 1.0 / 65536, 1.0 / 16)
+    secs = r.step()
+    return {"value": round(r.rows / secs), "unit": "rows/s", "cores": th, "kind": "port",
+            "sample": f"{r.rows} rows: every sweep case at {frac:.2e} of its rows (same mix), oracle on {th} "
+                      f"host threads, {secs:.1f} s"}
+
+
+def cpu_query(cpu_seconds):
+    th = threads_all()
+    r, rows = calibrate(lambda n: QueryRunner(int(n), th), cpu_seconds, 1 << 16, 1 << 28)
+    secs = r.step()
+    return {"value": round(r.rows / secs), "unit": "rows/s", "cores": th, "kind": "port",
+            "sample": f"{r.rows} rows of the same query (group ids given), oracle on {th} host threads, "
+                      f"{secs:.1f} s"}
+
+
+def cpu_batch(tasks, cpu_seconds):
+    th = threads_all()
+    r, frac = calibrate(lambda f: BatchRunner(tasks, f, th), cpu_seconds, 1.0 / 4096, 1.0 / 8)
+    secs = r.step()
+    return {"value": round(len(tasks) / (secs / frac), 4), "unit": "queries/s", "cores": th, "kind": "port",
+            "sample": f"{r.rows} rows: every task at {frac:.2e} of its rows in {secs:.1f} s, queries/s scaled to "
+                      f"full rows (time / fraction); oracle on {th} host threads"}
+
+
+def cpu_sin(cpu_seconds):
+    th = threads_all()
+    r, frac = calibrate(lambda f: SinRunner(f, th), cpu_seconds, 1.0 / 2048, 1.0 / 8)
+    secs = r.step()
+    return {"value": round(r.rows / secs), "unit": "rows/s", "cores": th, "kind": "port",
+            "sample": f"{r.rows} rows: every case at {frac:.2e} of its rows (same mix), oracle on {th} host "
+                      f"threads, {secs:.1f} s"}
+
+
+def cpu_filter(cpu_seconds):
+    th = threads_all()
+    r, rows = calibrate(lambda n: FilterRunner(int(n), th), cpu_seconds, 1 << 14, 1 << 26)
+    secs = r.step()
+    return {"value": round(r.rows / secs), "unit": "rows/s", "cores": th, "kind": "port",
+            "sample": f"{r.rows} rows of the same predicate and selection, oracle on {th} host threads, "
+                      f"{secs:.1f} s"}
+
+
+# ------------------------------------------------- output checks (oracle)
+def _host(t, a, b):
+    return bytes(t[a:b].cpu().numpy().tobytes())
+
+
+def verify_sweep(cases, mods, inputs, outs, slice_rows=1024):
+    """Three row ranges of every case (first, middle, last) recomputed by the
+    oracle from the same input bytes and compared byte for byte."""
+    orc = _oracle()
+    bad, checked = [], 0
+    for c, m, ins, o in zip(cases, mods, inputs, outs):
+        rows, ob = c["rows"], m.value_bytes
+        for off in sorted({0, max(0, rows // 2 - slice_rows // 2), max(0, rows - slice_rows)}):
+            r = min(slice_rows, rows - off)
+            cols = [_host(d.data, off * d.value_bytes, (off + r) * d.value_bytes) for d in ins]
+            exp, _ = orc.eval_expr(m.built, m.root, cols, r, ob)
+            checked += r
+            if _host(o, off * ob, (off + r) * ob) != exp:
+                bad.append(f"p={c['p']} {c['op']} rows {off}..{off + r}")
+    return {"ok": not bad, "rows_checked": checked, "mismatches": bad,
+            "how": "3 row ranges of 1024 per case vs the oracle on the same input bytes"}
+
+
+def verify_query_full(q, aggs, cols, k1, k2, outs, G):
+    """The whole query recomputed by the oracle from the same input bytes (group
+    ids from the key bytes in ascending key order) and compared byte for byte."""
+    import numpy as np
+    orc = _oracle()
+    rows = k1.numel()
+    key = k1.cpu().numpy().astype(np.int32) * 256 + k2.cpu().numpy().astype(np.int32)
+    uniq, gid = np.unique(key, return_inverse=True)
+    host = [_host(c, 0, c.numel()) for c in cols]
+    exp = orc.query(q.built, q.aggs, host, gid.astype(np.int32).tobytes(), rows, len(uniq), threads=threads_all())
+    bad = []
+    for i, ((kind, _), o, e) in enumerate(zip(aggs, outs, exp)):
+        if _host(o, 0, len(e)) != e:
+            bad.append(f"aggregate {i}")
+    return {"ok": not bad and len(uniq) == G, "rows_checked": rows, "mismatches": bad,
+            "how": "every row vs the oracle"}
+
+
+def verify_query_sums(cols, k1, k2, outs, aggs, G, chunk=1 << 24):
+    """Size-independent check of the full-size query: exact per-group integer
+    sums of the four columns and the two products (decoded and multiplied in
+    int64 by torch, chunk by chunk, then added as Python integers), COUNT, and
+    AVG by the divide rule, compared with the 133-byte images."""
+    import torch
+    from oracle import pyref
+    rows = k1.numel()
+    key_all = (k1.to(torch.int32) * 256 + k2.to(torch.int32))
+    uniq = torch.unique(key_all).tolist()
+    sums = [[0] * len(uniq) for _ in range(5)]
+    cnt = [0] * len(uniq)
+    w8 = torch.tensor([1 << (8 * i) for i in range(7)], dtype=torch.int64, device=k1.device)
+    lut = torch.full((65536,), -1, dtype=torch.int64, device=k1.device)
+    lut[torch.tensor(uniq, device=k1.device)] = torch.arange(len(uniq), device=k1.device)
+    for a in range(0, rows, chunk):
+        b = min(rows, a + chunk)
+        v = [(c[a * 7:b * 7].view(-1, 7).to(torch.int64) * w8).sum(1) for c in cols]  # unsigned (sign bit clear)
+        qty, price, disc, tax = v
+        dp = price * (100 - disc)
+        ch = dp * (100 + tax)
+        g = lut[key_all[a:b].to(torch.int64)]
+        for i, x in enumerate((qty, price, dp, ch, disc)):
+            s = torch.zeros(len(uniq), dtype=torch.int64, device=k1.device).index_add_(0, g, x)
+            for j in range(len(uniq)):
+                sums[i][j] += int(s[j])
+        cc = torch.bincount(g, minlength=len(uniq))
+        for j in range(len(uniq)):
+            cnt[j] += int(cc[j])
+    scales = [2, 2, 4, 6, 2]
+    src_of = {0: 0, 1: 1, 2: 2, 3: 3, 4: 0, 5: 1, 6: 4}
+    bad = []
+    for i, (kind, _) in enumerate(aggs):
+        o = outs[i][: len(uniq) * (8 if kind == 0 else 133)].cpu().numpy().tobytes()
+        for j in range(len(uniq)):
+            if kind == 0:
+                got = int.from_bytes(o[8 * j:8 * j + 8], "little", signed=True)
+                if got != cnt[j]:
+                    bad.append(f"COUNT group {j}")
+                continue
+            img = o[133 * j:133 * j + 133]
+            mag = int.from_bytes(img[5:133], "little")
+            s = sums[src_of[i]][j]
+            if kind == 1:
+                exp = (1, 0, scales[src_of[i]], s)
+            else:  # the divide rule (scale + 4, its 64-bit branch included) as oracle/pyref.py restates it
+                (sq, q, fq), _ = pyref.div((0, s, scales[src_of[i]]), (0, cnt[j], 0))
+                exp = (1, sq, fq, q)
+            if (img[0], img[1], img[3], mag) != exp:
+                bad.append(f"aggregate {i} group {j}")
+    return {"ok": not bad and len(uniq) == G and sum(cnt) == rows, "rows_checked": rows, "mismatches": bad,
+            "how": "exact per-group integer sums (torch int64 per chunk, Python integers across chunks)"}
+
+
+def verify_rows(m, cols, out, rows, slice_rows=64, n_slices=3):
+    """n_slices row ranges of a one-input-per-column expression output vs the oracle."""
+    orc = _oracle()
+    bad, checked = [], 0
+    offs = sorted({0, max(0, rows // 2 - slice_rows // 2), max(0, rows - slice_rows)}) if n_slices >= 3 else [0]
+    for off in offs:
+        r = min(slice_rows, rows - off)
+        host = [_host(d.data, off * d.value_bytes, (off + r) * d.value_bytes) for d in cols]
+        exp, _ = orc.eval_expr(m.built, m.root, host, r, m.value_bytes)
+        checked += r
+        if _host(out, off * m.value_bytes, (off + r) * m.value_bytes) != exp:
+            bad.append(f"rows {off}..{off + r}")
+    return bad, checked
 
 
 # ---------------------------------------------------------- reference arm
 def run_reference(args, rank, world):
     """The reference's decimal arithmetic has no CPU implementation (it is
-    device-only PTX); its restatement in oracle/ runs on all host cores."""
+    device-only PTX); its restatement in oracle/ runs on all host cores.
+    Every step is a bounded sample of the workload, timed; the record's config
+    is the one our arm reports for the same workload.  Only the oracle's
+    library is loaded in this process (typing and the byte table included)."""
     if rank != 0:
         return None
-    threads = os.cpu_count() or 1
-    if args.workload in ("serve", "text"):
+    from ultraprecise_b200 import abi, codec
+    orc = _oracle()
+    codec.compact_bytes = orc.compact_bytes  # the oracle's byte table for every workload helper here
+    th = threads_all()
+    if args.workload in ("serve", "text", "costmodel"):
         return {"impl": "reference", "unavailable": "no CPU counterpart timed for this workload; the reference's "
                                                     "CPU decimal path is timed by the other workloads"}
-    if args.workload == "sin":
-        per = args.cpu_seconds / max(1, args.steps)
-        rates, sample = [], ""
-        for k in range(max(1, args.steps)):
-            r, sample = sin_cpu_rate(per, threads, seed=11 + k)
-            rates.append(r)
-        rate = sorted(rates)[len(rates) // 2]
-        from ultraprecise_b200 import workloads
-        total = sum(r for _, r in workloads.SIN)
-        return {"metric": SIN_METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": round(total / rate * 1e3, 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-                "impl": "reference", "config": {"workload": "sin series on host cores, bounded sample",
-                                                "parallelism": f"{threads} host threads"},
-                "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
+    K, W = max(1, args.steps), max(0, args.warmup)
+    budget = args.ref_seconds
+
+    def record(runner, what, metric, unit, config, sample, scale_to_full=1.0):
+        for _ in range(W):
+            runner.step()
+        secs = [runner.step() for _ in range(K)]
+        mean = sum(secs) / len(secs)
+        value = (runner.rows / mean) if unit == "rows/s" else (what / (mean / scale_to_full))
+        value = round(value) if unit == "rows/s" else round(value, 4)
+        return {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": round(mean * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic", "impl": "reference",
+                "config": config,
+                "sample": sample,
+                "cpu_baseline": {"value": round(value, 4), "unit": unit, "cores": th, "kind": "port",
                                  "sample": sample},
-                "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if args.workload == "filter":
-        rate, rows = filter_cpu_rate(args.cpu_seconds, threads)
-        return {"metric": FILTER_METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": 1, "steps": args.steps,
-                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "u32 limbs (exact decimal)", "data": "synthetic", "impl": "reference",
-                "config": {"workload": "predicate + row selection on host cores, bounded sample", "rows": rows},
-                "cpu_baseline": {"kind": "port", "cores": threads, "value": round(rate),
-                                 "sample": f"{rows} rows of the predicate and selection"},
-                "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if args.workload == "query":
-        per = args.cpu_seconds / max(1, args.steps)
-        rates, rows = [], 0
-        for k in range(max(1, args.steps)):
-            r, rows = query_cpu_rate(per, threads, seed=3 + k)
-            rates.append(r)
-        rate = sorted(rates)[len(rates) // 2]
-        return {"metric": QUERY_METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": round((256 << 20) / rate * 1e3, 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-                "impl": "reference", "config": {"workload": "grouped query on host cores, bounded sample",
-                                                "parallelism": f"{threads} host threads"},
-                "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
-                                 "sample": f"{rows} rows per step"},
-                "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if args.workload == "batch":
-        tasks, _ = batch_setup(rank)
-        per = args.cpu_seconds / max(1, args.steps)
-        rates, rows, frac = [], 0, 0.0
-        for k in range(max(1, args.steps)):
-            r, frac, rows = batch_cpu_rate(tasks, per, threads, seed=1 + k)
-            rates.append(r)
-        rate = sorted(rates)[len(rates) // 2]
-        return {"metric": BATCH_METRIC, "value": round(rate, 4), "unit": "queries/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(len(tasks) / rate * 1e3, 3),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "u32 limbs (exact decimal)", "data": "synthetic", "impl": "reference",
-                "config": {"workload": "64-task batched mixed precision on host cores, bounded sample",
-                           "parallelism": f"{threads} host threads"},
-                "cpu_baseline": {"value": round(rate, 4), "unit": "queries/s", "cores": threads, "kind": "port",
-                                 "sample": f"{rows} rows per step: every task at {frac:.2e} of its rows"},
-                "e2e": {"value": round(rate, 4), "unit": "queries/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-    cases = sweep_cases()
-    per = args.cpu_seconds / max(1, args.steps)
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_rate(cases, min(per, 2.0), threads, seed=99)
-    rates, rows = [], 0
-    for k in range(max(1, args.steps)):
-        r, frac, rows = cpu_rate(cases, per, threads, seed=1 + k)
-        rates.append(r)
-    rate = sorted(rates)[len(rates) // 2]
-    total_rows = sum(c["rows"] for c in cases)
-    return {"metric": METRIC, "value": round(rate), "unit": "rows/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(total_rows / rate * 1e3, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact decimal)", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": "precision sweep on host cores, bounded sample",
-                       "parallelism": f"{threads} host threads"},
-            "cpu_baseline": {"value": round(rate), "unit": "rows/s", "cores": threads, "kind": "port",
-                             "sample": f"{rows} rows per step: every sweep case at {frac:.2e} of its rows"},
-            "e2e": {"value": round(rate), "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "e2e": {"value": round(value, 4), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+    def per_step(share):
+        return max(0.2, min(4.0, budget * share / (K + W)))
+
+    def sweep_rec():
+        cases = sweep_cases(compact_bytes=orc.compact_bytes)
+        r, frac = calibrate(lambda f: SweepRunner(cases, f, th), per_step(0.4), 1.0 / 65536, 1.0 / 16)
+        full = sum(c["rows"] for c in cases)
+        return record(r, r.rows, METRIC, "rows/s", sweep_config(world, full),
+                      f"each step: {r.rows} rows, every sweep case at {frac:.2e} of its rows, oracle on {th} "
+                      f"host threads")
+
+    def query_rec():
+        r, rows = calibrate(lambda n: QueryRunner(int(n), th), per_step(0.2), 1 << 16, 1 << 28)
+        return record(r, r.rows, QUERY_METRIC, "rows/s", query_config(world, 256 << 20),
+                      f"each step: {r.rows} rows of the query (group ids given), oracle on {th} host threads")
+
+    def batch_rec():
+        tasks, redraws = batch_setup(rank)
+        r, frac = calibrate(lambda f: BatchRunner(tasks, f, th), per_step(0.2), 1.0 / 4096, 1.0 / 8)
+        full = sum(t["rows"] for t in tasks)
+        return record(r, len(tasks), BATCH_METRIC, "queries/s", batch_config(world, full, redraws),
+                      f"each step: every task at {frac:.2e} of its rows ({r.rows} rows); queries/s scaled to full "
+                      f"rows (time / fraction); oracle on {th} host threads", scale_to_full=frac)
+
+    def sin_rec():
+        from ultraprecise_b200 import workloads
+        r, frac = calibrate(lambda f: SinRunner(f, th), per_step(0.2), 1.0 / 2048, 1.0 / 8)
+        full = sum(rr for _, rr in workloads.SIN)
+        return record(r, r.rows, SIN_METRIC, "rows/s", sin_config(world, full),
+                      f"each step: {r.rows} rows, every case at {frac:.2e} of its rows, oracle on {th} host "
+                      f"threads")
+
+    def filter_rec():
+        r, rows = calibrate(lambda n: FilterRunner(int(n), th), per_step(1.0), 1 << 14, 1 << 26)
+        return record(r, r.rows, FILTER_METRIC, "rows/s", filter_config(world, 64 << 20),
+                      f"each step: {r.rows} rows of the predicate and selection, oracle on {th} host threads")
+
+    one = {"sweep": sweep_rec, "query": query_rec, "batch": batch_rec, "sin": sin_rec, "filter": filter_rec}
+    if args.workload in one:
+        res = one[args.workload]()
+    else:  # all: the sweep is the headline, the other configs ride along
+        res = sweep_rec()
+        res["configs"] = {"0_grouped_query": query_rec(), "2_batch": batch_rec(), "3_sin": sin_rec(),
+                          "4_serve": {"impl": "reference", "unavailable": "served stream has no CPU counterpart"}}
+    if abi._lib is not None:
+        raise SystemExit("reference arm loaded the product library")
+    return res
+
+
+# ------------------------------------------------------- cost model
+COSTMODEL_METRIC = "held-out launch time with threads per value chosen by the learned cost model vs the width rule"
+
+
+def run_costmodel(args, rank, world):
+    """The learned cost model end to end: launch times of the training shapes
+    measured on the device, the network trained on the GPU by the library's
+    kernels, then threads per value chosen for held-out shapes (other
+    precisions, other expressions) by the model and by the width rule, each
+    choice timed.  value = total held-out time under the rule / under the
+    model (higher is better; 1.0 = no gain)."""
+    import numpy as np
+    import torch
+    from ultraprecise_b200 import costmodel, workloads
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    with ClockSampler(dev) as clk:
+        X, y, recs, collect_s = costmodel.collect_samples(workloads.costmodel_train_shapes(),
+                                                          workloads.COSTMODEL_ROWS)
+        m = costmodel.CostModel(seed=3)
+        t0 = time.perf_counter()
+        loss = m.train(X, y, epochs=400, batch=64, lr=3e-3, seed=5)
+        train_s = time.perf_counter() - t0
+        rows = 1 << 20
+        tot = {"model": 0.0, "rule": 0.0, "best": 0.0}
+        per, err = [], []
+        for name, e, cols in workloads.costmodel_eval_shapes():
+            p = cols[0].precision
+            data = [runtime_col(rows, p, cols[k].scale, 900 + k) for k in range(len(cols))]
+            times = {}
+            for t in costmodel.TPV_CHOICES:
+                times[t] = costmodel.time_launch(compile_tpv(e, cols, t), data, rows, reps=5)
+            costmodel.CostModel.clear_default()
+            rule_t = compile_tpv(e, cols, 0).threads_per_value
+            model_t, pred = m.choose_tpv(e, cols, rows)
+            f = np.stack([costmodel.features(e, cols, t, rows)[0] for t in costmodel.TPV_CHOICES])
+            lp = m.predict(f)
+            err += [abs(float(lp[i]) - math.log(times[t])) for i, t in enumerate(costmodel.TPV_CHOICES)]
+            tot["model"] += times[model_t]
+            tot["rule"] += times[rule_t]
+            tot["best"] += min(times.values())
+            per.append({"shape": name, "rule_tpv": rule_t, "model_tpv": model_t,
+                        "best_tpv": min(times, key=times.get),
+                        "ms": {str(k): round(v, 4) for k, v in times.items()}})
+            del data
+    gain = tot["rule"] / tot["model"]
+    return {"metric": COSTMODEL_METRIC, "value": round(gain, 4), "unit": "x (rule time / model time)",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 network; u32 limbs (exact decimal) kernels", "data": "synthetic",
+            "config": {"workload": "train on 25 shapes (5 expressions x p 40..600) x 6 threads-per-value x 3 row "
+                                   "counts; judge on 12 held-out shapes (3 other expressions x p 60..450) at 1M rows"},
+            "train": {"samples": int(len(y)), "collect_s": round(collect_s, 2), "train_s": round(train_s, 3),
+                      "epochs": 400, "batch": 64, "final_mse_standardised": round(loss, 5),
+                      "kernel": "k_mlp_step (forward + backward + Adam, one CTA per step)"},
+            "held_out_ms": {k: round(v, 4) for k, v in tot.items()},
+            "regret_vs_best": round(tot["model"] / tot["best"], 4),
+            "held_out_log_ms_mae": round(float(np.mean(err)), 4), "shapes": per, "clocks": clk.summary(),
+            "gpu_launches": None}
+
+
+def runtime_col(rows, p, s, seed):
+    from ultraprecise_b200 import runtime
+    return runtime.DeviceColumn(runtime.gen_digits(rows, p, seed, nonzero=True), p, s)
+
+
+def compile_tpv(e, cols, tpv):
+    from ultraprecise_b200 import runtime
+    return runtime.compile_expr(e, cols, threads_per_value=tpv)
+
+
+# ------------------------------------------------------- all configs
+def run_all(args, rank, world):
+    """The default run: the precision sweep is the headline record; the
+    grouped query (1M and 256M rows), the 64-task batch, the sin series and a
+    short served stream follow as sub-records under "configs", each with its
+    own roofline, e2e, output check and CPU baseline."""
+    import gc
+    import torch
+    res = run_ours(args, rank, world)
+    res["configs"] = {}
+    for name, fn in (("0_grouped_query", run_query), ("2_batch", run_batch), ("3_sin", run_sin),
+                     ("4_serve", run_serve), ("5_costmodel", run_costmodel)):
+        gc.collect()
+        torch.cuda.empty_cache()
+        t = time.perf_counter()
+        sub = fn(args, rank, world)
+        sub["wall_s"] = round(time.perf_counter() - t, 1)
+        res["configs"][name] = sub
+    res["configs"]["1_sweep"] = "the headline record itself"
+    return res
 
 
 # ---------------------------------------------------------- distributed
@@ -1379,8 +1741,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     run = {"batch": run_batch, "query": run_query, "sin": run_sin, "serve": run_serve, "text": run_text,
-           "filter": run_filter}.get(
-        args.workload, run_ours)
+           "filter": run_filter, "sweep": run_ours, "costmodel": run_costmodel}.get(args.workload, run_all)
     res = run(args, rank, world)
     if world > 1:
         import torch.distributed as dist
