@@ -176,6 +176,13 @@ static void digits(Rng& g, u32 (&a)[N], int p) {
     }
 }
 
+// 10^k modulo 2^64
+constexpr uint64_t pow10_mod64(int k) {
+    uint64_t v = 1;
+    for (int i = 0; i < k; i++) v *= 10u;
+    return v;
+}
+
 template <int NA, int NP, u32 SHIFT, uint64_t P10W>
 static long check_div_round(Rng& g, long n, int p, int s) {
     constexpr int NR = NA + NP + 1;
@@ -240,5 +247,8 @@ int main(int argc, char** argv) {
     bad += check_div_round<2, 1, 8u, 100000000ull>(g, n, 18, 4);
     bad += check_div_round<4, 2, 13u, 10000000000000ull>(g, n, 38, 9);
     bad += check_div_round<8, 3, 23u, 0x2c7e14af6800000ull>(g, n / 2, 76, 19);
+    bad += check_div_round<16, 5, 41u, pow10_mod64(41)>(g, n / 8, 150, 37);
+    bad += check_div_round<32, 9, 79u, pow10_mod64(79)>(g, n / 32, 300, 75);
+    bad += check_div_round<63, 17, 154u, pow10_mod64(154)>(g, n / 128, 600, 150);
     return bad ? 1 : 0;
 }

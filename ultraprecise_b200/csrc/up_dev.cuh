@@ -195,13 +195,16 @@ template <int N>
 UP_DI void shl_bits(u32 (&r)[N], const u32 (&a)[N], u32 s) {
     u32 t[N];
     copy_ext(t, a);
-    // limb shift by s/32, done as a barrel of static shifts
+    // limb shift by s/32, done as a barrel of static shifts (skipped as a
+    // whole when s < 32, the usual case of a normalising shift)
     const u32 ls = s >> 5;
+    if (ls != 0u) {
 #pragma unroll
-    for (int k = 1; k < N; k <<= 1) {
-        if (ls & (u32)k) {
+        for (int k = 1; k < N; k <<= 1) {
+            if (ls & (u32)k) {
 #pragma unroll
-            for (int i = N - 1; i >= 0; i--) t[i] = i >= k ? t[i >= k ? i - k : 0] : 0u;
+                for (int i = N - 1; i >= 0; i--) t[i] = i >= k ? t[i >= k ? i - k : 0] : 0u;
+            }
         }
     }
     const u32 bs = s & 31u;
@@ -215,11 +218,13 @@ UP_DI void shr_bits(u32 (&r)[N], const u32 (&a)[N], u32 s) {
     u32 t[N];
     copy_ext(t, a);
     const u32 ls = s >> 5;
+    if (ls != 0u) {
 #pragma unroll
-    for (int k = 1; k < N; k <<= 1) {
-        if (ls & (u32)k) {
+        for (int k = 1; k < N; k <<= 1) {
+            if (ls & (u32)k) {
 #pragma unroll
-            for (int i = 0; i < N; i++) t[i] = i + k < N ? t[i + k < N ? i + k : 0] : 0u;
+                for (int i = 0; i < N; i++) t[i] = i + k < N ? t[i + k < N ? i + k : 0] : 0u;
+            }
         }
     }
     const u32 bs = s & 31u;
@@ -339,12 +344,14 @@ UP_DI u32 knuth_step(u32 (&w)[NB + 1], const u32 (&bn)[NB], u32 qhat) {
 
 // Knuth, TAOCP vol. 2, 4.3.1, Algorithm D in base 2^32 with static array
 // sizes: the divisor is normalised to exactly NB limbs (top bit set) by a
-// dynamic left shift applied to both operands; the nx - nb + 1 quotient
+// dynamic left shift s applied to both operands; the nx - nb + 1 quotient
 // digits that can be nonzero are produced (nx, nb: the operands' significant
-// limbs), each estimated by QuotEst.  q = floor(x / b), rem = x mod b.
-// Requires b != 0.
+// limbs), each estimated by QuotEst.  q = floor(x / b); rn = (x mod b) << s
+// and bn = b << s (the normalised remainder and divisor, which is all a
+// rounding decision needs).  Requires b != 0.
 template <int NX, int NB>
-UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&b)[NB]) {
+UP_DI void divmod_norm(u32 (&q)[NX], u32 (&rn)[NB], u32 (&bn)[NB], u32& s, const u32 (&x)[NX],
+                       const u32 (&b)[NB]) {
     if constexpr (NB == 1) {
         const u32 sh = (u32)__clz(b[0]);
         const u32 d = b[0] << sh;
@@ -355,19 +362,50 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
             const u32 lo = sh ? __funnelshift_l(i > 0 ? x[i > 0 ? i - 1 : 0] : 0u, x[i], sh) : x[i];
             q[i] = div2by1(r, lo, d, v, r);
         }
-        rem[0] = r >> sh;
+        rn[0] = r;
+        bn[0] = d;
+        s = sh;
     } else {
     // the shift reaches past a limb when b's value is narrower than NB limbs
     constexpr int NU = NX + NB + 1;
+    constexpr bool kUnroll = (NX + 1) * NB <= 96;
     const u32 bl = bitlen(b);
-    const u32 s = 32u * NB - bl;  // normalising shift
-    u32 bn[NB];
-    shl_bits(bn, b, s);
+    s = 32u * NB - bl;  // normalising shift
     u32 un[NU];
-    {
+    if constexpr (kUnroll) {
+        shl_bits(bn, b, s);
         u32 xe[NU];
         copy_ext(xe, x);
         shl_bits(un, xe, s);
+    } else {
+        // Wide operands: un is indexed by the digit loop (local memory), so
+        // it is written limb by limb at its shifted position, and a limb
+        // shift of b (a divisor narrower than NB limbs) goes through a local
+        // copy; a barrel of static shifts would hold several copies of the
+        // operands in registers at once.
+        const u32 ls = s >> 5, bs = s & 31u;
+        for (int i = 0; i < NU; i++) un[i] = 0u;
+#pragma unroll
+        for (int i = 0; i <= NX; i++) {
+            const u32 hi = i < NX ? x[i < NX ? i : 0] : 0u;
+            const u32 lo = i > 0 ? x[i > 0 ? i - 1 : 0] : 0u;
+            un[i + ls] = __funnelshift_l(lo, hi, bs);
+        }
+        if (ls == 0u) {
+#pragma unroll
+            for (int i = 0; i < NB; i++) bn[i] = __funnelshift_l(i > 0 ? b[i > 0 ? i - 1 : 0] : 0u, b[i], bs);
+        } else {
+            u32 bt[NB];
+#pragma unroll
+            for (int i = 0; i < NB; i++) bt[i] = b[i];
+#pragma unroll
+            for (int i = 0; i < NB; i++) {
+                const int k = i - (int)ls;
+                const u32 hi = k >= 0 ? bt[k >= 0 ? k : 0] : 0u;
+                const u32 lo = k >= 1 ? bt[k >= 1 ? k - 1 : 0] : 0u;
+                bn[i] = __funnelshift_l(lo, hi, bs);
+            }
+        }
     }
     QuotEst est;
     est.init(bn[NB - 1], bn[NB - 2]);
@@ -375,32 +413,52 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
     const int jmax = (int)((bitlen(x) + 31u) >> 5) - (int)((bl + 31u) >> 5);
 #pragma unroll
     for (int i = 0; i < NX; i++) q[i] = 0u;
-    if (jmax < 0) {  // x < b
-        copy_ext(rem, x);
+    if (jmax < 0) {  // x < b: the remainder is x itself
+#pragma unroll
+        for (int i = 0; i < NB; i++) rn[i] = un[i];
         return;
     }
-    constexpr bool kUnroll = (NX + 1) * NB <= 96;
-    if constexpr (!kUnroll && NB <= 40) {
+    if constexpr (!kUnroll && NB <= 64) {
         // Wide operands: the rolled loop keeps the current remainder window
         // un[j .. j+NB] in registers (static indices) and moves it down one
-        // limb per quotient digit, reading a single dividend limb per step.
+        // limb per quotient digit, reading a single dividend limb per step
+        // (up to 40 limbs two digits per iteration, so that half the moves
+        // are renamings; wider windows one digit at a time, for registers).
         u32 w[NB + 1];
 #pragma unroll
         for (int i = 0; i <= NB; i++) w[i] = un[jmax + i];
+        int j = jmax;
+        if constexpr (NB > 40) {
 #pragma unroll 1
-        for (int j = jmax; j >= 0; j--) {
-            const u32 qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
-            if (j < NX) q[j < NX ? j : 0] = qd;
-            if (j > 0) {
+            for (; j >= 1; j--) {
+                q[j < NX ? j : 0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
                 for (int i = NB; i > 0; i--) w[i] = w[i - 1];
                 w[0] = un[j - 1];
             }
-        }
-        u32 rl[NB];
+            q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
-        for (int i = 0; i < NB; i++) rl[i] = w[i];
-        shr_bits(rem, rl, s);
+            for (int i = 0; i < NB; i++) rn[i] = w[i];
+            return;
+        }
+#pragma unroll 1
+        for (; j >= 1; j -= 2) {
+            u32 qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+            q[j < NX ? j : 0] = qd;
+#pragma unroll
+            for (int i = NB; i > 0; i--) w[i] = w[i - 1];
+            w[0] = un[j - 1];
+            qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+            q[j - 1] = qd;
+            if (j >= 2) {
+#pragma unroll
+                for (int i = NB; i > 0; i--) w[i] = w[i - 1];
+                w[0] = un[j - 2];
+            }
+        }
+        if (j == 0) q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+#pragma unroll
+        for (int i = 0; i < NB; i++) rn[i] = w[i];
         return;
     }
     // Static window positions: digit j uses un[j .. j+NB], j <= jmax <= NX - 1.
@@ -415,12 +473,18 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
         for (int i = 0; i <= NB; i++) un[j + i] = w[i];
         q[j] = qd;
     }
-    u32 rl[NB];
+    // the remainder (< bn) sits in un[0..NB)
 #pragma unroll
-    for (int i = 0; i < NB; i++) rl[i] = un[i];
-    // the remainder (< bn) sits in un[0..NB); undo the normalising shift
-    shr_bits(rem, rl, s);
+    for (int i = 0; i < NB; i++) rn[i] = un[i];
     }
+}
+
+// q = floor(x / b), rem = x mod b.  Requires b != 0.
+template <int NX, int NB>
+UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&b)[NB]) {
+    u32 rn[NB], bn[NB], s;
+    divmod_norm(q, rn, bn, s, x, b);
+    shr_bits(rem, rn, s);  // undo the normalising shift
 }
 
 // Bit length of 10^k estimated the way the reference does before choosing
@@ -468,15 +532,22 @@ UP_DI u32 div_round(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32
     u32 x[NX];
     mul(x, a, p10);
     u32 q[NX];
-    u32 rem[NB];
-    divmod(q, rem, x, b);
     bool up;
     if (hds <= 32u) {
-        up = (u32)(rem[0] * 2u) >= b[0];
+        // one-limb divisor: 2/1 steps, whatever NB is; the reference doubles
+        // this remainder modulo 2^32
+        const u32 b1[1] = {b[0]};
+        u32 r1[1];
+        divmod<NX, 1>(q, r1, x, b1);
+        up = (u32)(r1[0] * 2u) >= b[0];
     } else {
+        // 2 * rem >= b  <=>  2 * (rem << s) >= (b << s): decided on the
+        // normalised remainder and divisor, so b itself is not kept
+        u32 rn[NB], bn[NB], s;
+        divmod_norm(q, rn, bn, s, x, b);
         u32 dbl[NB + 1];
-        add(dbl, rem, rem);
-        up = cmp(dbl, b) >= 0;
+        add(dbl, rn, rn);
+        up = cmp(dbl, bn) >= 0;
     }
     copy_ext(r, q);
     if (up) add_small(r, 1u);

@@ -143,6 +143,13 @@ def prune(verbose: bool = False) -> None:
 
 if __name__ == "__main__":
     import sys
+    try:
+        # The benchmark and test processes import torch before the library,
+        # so they run torch's NVRTC; compiling with the same one keeps the
+        # cache keys (which name the NVRTC version) theirs.
+        import torch  # noqa: F401
+    except ImportError:
+        pass
     if "--prune" in sys.argv:
         prune(verbose="-v" in sys.argv)
     elif "--compress" in sys.argv:
