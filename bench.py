@@ -392,7 +392,7 @@ def batch_setup(rank):
 
 def run_batch(args, rank, world):
     import torch
-    from ultraprecise_b200 import abi, batch, runtime, workloads
+    from ultraprecise_b200 import abi, batch, codec, runtime, workloads
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     lib = abi.load()
@@ -402,9 +402,6 @@ def run_batch(args, rank, world):
     madd_peak = C.c_double(0)
     abi.check(lib.up_util_imad_peak(C.byref(madd_peak), stream.cuda_stream), "imad peak")
     specs = workloads.batch_specs(tasks)
-    t_build = time.perf_counter()
-    b = batch.Batch(specs, autotune=True, use_graph=True)
-    build_s = time.perf_counter() - t_build
     with torch.cuda.stream(stream):
         data = workloads.batch_columns(tasks, seed=20261203 + 1000003 * rank)
     torch.cuda.synchronize()
@@ -414,24 +411,39 @@ def run_batch(args, rank, world):
         dc = [runtime.DeviceColumn(c, t["p"], t["s"]) for c in cols]
         devcols.append(dc)
         if t["agg"] < 0:
-            vb = b.task_type(k)[2]
-            t["out_bytes_per_row"] = vb
-            o = torch.empty(max(1, rows * vb), dtype=torch.uint8, device="cuda")
-            b.bind(k, dc, rows, o)
+            t["out_bytes_per_row"] = codec.compact_bytes(workloads_root_precision(t))
+            o = torch.empty(max(1, rows * t["out_bytes_per_row"]), dtype=torch.uint8, device="cuda")
             gids.append(None)
         else:
             t["out_bytes_per_row"] = 4  # the group id read
-            g = torch.from_numpy(gid).cuda()
+            gids.append(torch.from_numpy(gid).cuda())
             o = torch.empty(t["groups"] * abi.UP_AGG_DECIMAL_BYTES, dtype=torch.uint8, device="cuda")
-            b.bind(k, dc, rows, o, g, t["groups"])
-            gids.append(g)
         out_bytes += o.numel()
         outs.append(o)
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
-    t_tune = time.perf_counter()
-    b.launch(err, stream=stream)  # tunes (or loads the tuned shapes) and captures the graph
-    torch.cuda.synchronize()
-    tune_s = time.perf_counter() - t_tune
+
+    def make(policy, model=None):
+        """A batch over the bound tasks with one threads-per-value policy:
+        (batch, build s, tune + capture s)."""
+        if model is not None:
+            model.set_default()
+        try:
+            t0 = time.perf_counter()
+            bb = batch.Batch(specs, autotune=True, use_graph=True, tpv_policy=policy)
+            t1 = time.perf_counter()
+        finally:
+            if model is not None:
+                model.clear_default()
+        for k, t in enumerate(tasks):
+            if t["agg"] < 0:
+                bb.bind(k, devcols[k], data[k][0], outs[k])
+            else:
+                bb.bind(k, devcols[k], data[k][0], outs[k], gids[k], t["groups"])
+        bb.launch(err, stream=stream)  # tunes (or loads the tuned choices) and captures the graph
+        torch.cuda.synchronize()
+        return bb, t1 - t0, time.perf_counter() - t1
+
+    b, build_s, tune_s = make(batch.TPV_MEASURED)
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -449,6 +461,26 @@ def run_batch(args, rank, world):
     with ClockSampler(dev) as clk:
         ms_batch = timed(lambda: b.launch(err, stream=stream), args.steps, args.warmup)
     clocks = clk.summary()
+    tpv_measured = [b.task_tpv(k) for k in range(len(tasks))]
+    outs_measured = [o.clone() for o in outs]
+
+    # ablation of the threads-per-value choice of projection tasks: one thread
+    # per value, the width rule, the learned cost model (trained on the GPU by
+    # the library's kernels on shapes other than these tasks), measured
+    ablation = {}
+    for name, policy, model in (("one_thread", batch.TPV_ONE, None), ("width_rule", batch.TPV_AUTO, None),
+                                ("cost_model", batch.TPV_AUTO, trained_costmodel())):
+        bb, _, _ = make(policy, model)
+        ms = timed(lambda: bb.launch(err, stream=stream), max(3, args.steps // 2), args.warmup)
+        torch.cuda.synchronize()
+        tv = [bb.task_tpv(k) for k in range(len(tasks))]
+        ablation[name] = {"ms_per_step": round(ms, 4), "cooperative_tasks": sum(1 for x in tv if x > 1),
+                          "tpv": tv, "byte_equal": all(torch.equal(a, c) for a, c in zip(outs, outs_measured))}
+        del bb
+    ablation["measured"] = {"ms_per_step": round(ms_batch, 4),
+                            "cooperative_tasks": sum(1 for x in tpv_measured if x > 1), "tpv": tpv_measured}
+    for o, m in zip(outs, outs_measured):
+        o.copy_(m)
 
     # the same 64 tasks, one plain launch each (no synchronisation between them)
     plain = []
@@ -505,6 +537,7 @@ def run_batch(args, rank, world):
                         "traffic": None, "kernel": "up_batch band kernels (whole graph)",
                         "peak_source": "measured (up_util_imad_peak)", "hbm_achieved_gbs": round(gbs, 1),
                         "hbm_frac": round(gbs / hbm_peak, 4)},
+           "threads_per_value": ablation,
            "shapes": shapes, "module_build_s": round(build_s, 2), "tune_and_capture_s": round(tune_s, 2),
            "gpu_launches": args.steps * (1 + sum(1 for i in range(3) if any(
                b.task_type(k)[3] == i for k in range(n)))), "clocks": clocks}
@@ -512,11 +545,40 @@ def run_batch(args, rank, world):
         res["e2e"] = e2e_batch(args, b, tasks, data, outs, gids, world, stream)
     if not args.no_cpu_baseline:
         res["verified"] = verify_batch(tasks, data, outs)
+        same = same and all(v.get("byte_equal", True) for v in ablation.values())
         if not res["verified"]["ok"] or not same:
             raise SystemExit("batch outputs differ: " + json.dumps(res["verified"]) + f" plain_equal={same}")
         if rank == 0 and world == 1:
             res["cpu_baseline"] = cpu_batch(tasks, args.cpu_seconds)
     return res
+
+
+def workloads_root_precision(t):
+    """Precision of a projection task's result (the library's typing)."""
+    from ultraprecise_b200 import expr as E
+    b = E.build([t["expr"]], t["cols"])
+    E.derive_types(b)
+    return b.nodes[b.roots[0]].precision
+
+
+_COSTMODEL = {}
+
+
+def trained_costmodel():
+    """The cost model of this process: launch times of the training shapes
+    measured on the device, the network trained on the GPU by the library's
+    kernels (once; the batch ablation and the cost-model record share it)."""
+    if "m" not in _COSTMODEL:
+        from ultraprecise_b200 import costmodel, workloads
+        t0 = time.perf_counter()
+        X, y, recs, collect_s = costmodel.collect_samples(workloads.costmodel_train_shapes(),
+                                                          workloads.COSTMODEL_ROWS)
+        m = costmodel.CostModel(seed=3)
+        t1 = time.perf_counter()
+        loss = m.train(X, y, epochs=400, batch=64, lr=3e-3, seed=5)
+        _COSTMODEL.update(m=m, samples=int(len(y)), collect_s=collect_s, train_s=time.perf_counter() - t1,
+                          loss=loss, wall_s=time.perf_counter() - t0)
+    return _COSTMODEL["m"]
 
 
 def batch_config(world, rows, redraws):
@@ -1632,12 +1694,9 @@ def run_costmodel(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     with ClockSampler(dev) as clk:
-        X, y, recs, collect_s = costmodel.collect_samples(workloads.costmodel_train_shapes(),
-                                                          workloads.COSTMODEL_ROWS)
-        m = costmodel.CostModel(seed=3)
-        t0 = time.perf_counter()
-        loss = m.train(X, y, epochs=400, batch=64, lr=3e-3, seed=5)
-        train_s = time.perf_counter() - t0
+        m = trained_costmodel()
+        collect_s, train_s, loss = _COSTMODEL["collect_s"], _COSTMODEL["train_s"], _COSTMODEL["loss"]
+        y_n = _COSTMODEL["samples"]
         rows = 1 << 20
         tot = {"model": 0.0, "rule": 0.0, "best": 0.0}
         per, err = [], []
@@ -1666,7 +1725,7 @@ def run_costmodel(args, rank, world):
             "dtype": "fp32 network; u32 limbs (exact decimal) kernels", "data": "synthetic",
             "config": {"workload": "train on 25 shapes (5 expressions x p 40..600) x 6 threads-per-value x 3 row "
                                    "counts; judge on 12 held-out shapes (3 other expressions x p 60..450) at 1M rows"},
-            "train": {"samples": int(len(y)), "collect_s": round(collect_s, 2), "train_s": round(train_s, 3),
+            "train": {"samples": y_n, "collect_s": round(collect_s, 2), "train_s": round(train_s, 3),
                       "epochs": 400, "batch": 64, "final_mse_standardised": round(loss, 5),
                       "kernel": "k_mlp_step (forward + backward + Adam, one CTA per step)"},
             "held_out_ms": {k: round(v, 4) for k, v in tot.items()},

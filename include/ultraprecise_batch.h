@@ -37,7 +37,11 @@ typedef struct up_batch_opts {
     int32_t ctas_per_sm;       /* 0 = default */
     int32_t tile_rows;         /* 0 = default rows per work item */
     int32_t use_graph;         /* 1: capture the step once as a CUDA graph and replay it */
-    int32_t reserved;          /* 0 */
+    int32_t tpv_policy;        /* threads per value of projection tasks (aggregate tasks run one thread per
+                                  value): 0 = automatic (the default cost model's choice when one is set,
+                                  else the width rule); 1 = one thread per value; 2 = measured: the first
+                                  launch times each projection task alone at every candidate threads per
+                                  value on its bound inputs and keeps the fastest (cached on disk) */
     int64_t solo_rows;         /* tasks with at least this many rows run as their own kernels inside the
                                   same step (on forked streams); 0 = 262144, < 0 = never */
 } up_batch_opts;
@@ -68,6 +72,15 @@ up_status up_batch_shape(const up_batch* b, int32_t band, int32_t* block_threads
 /* Band (0..2) of a task and the result type of a projection task. */
 up_status up_batch_task_type(const up_batch* b, int32_t task, int32_t* precision, int32_t* scale,
                              int32_t* value_bytes, int32_t* band);
+
+/* Pin a projection task's threads per value (1, 2, 4, 8, 16 or 32; an
+ * expression without a cooperative form stays at 1).  The module is rebuilt
+ * on the next launch; the measured policy leaves pinned tasks alone. */
+up_status up_batch_set_task_tpv(up_batch* b, int32_t task, int32_t threads_per_value);
+
+/* Threads per value a task runs with (after the first launch under the
+ * measured policy). */
+up_status up_batch_task_tpv(const up_batch* b, int32_t task, int32_t* threads_per_value);
 
 void up_batch_release(up_batch* b);
 

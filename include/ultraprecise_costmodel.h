@@ -79,6 +79,17 @@ up_status up_costmodel_choose_tpv(up_costmodel* m, const up_expr_node* nodes, in
                                   const up_col_type* cols, int32_t n_cols, int64_t rows, int32_t* tpv,
                                   float* pred_ms);
 
+/* Ensembles: add a copy of `other`'s trained network (and standardisation)
+ * to `m`; predictions then average the log ms of m's network and every
+ * member (independently trained networks disagree where data is thin). */
+up_status up_costmodel_add_member(up_costmodel* m, const up_costmodel* other);
+
+/* Guard the choice: up_costmodel_choose_tpv keeps the width rule's threads
+ * per value unless the model predicts the best choice saves at least
+ * `margin` (0 <= margin < 1) of the rule's time.  0 (the default): the
+ * model's lowest prediction. */
+up_status up_costmodel_set_guard(up_costmodel* m, float margin);
+
 /* Make `m` (or NULL: none) the model that up_module_compile consults when
  * opts->threads_per_value is 0 (automatic): the threads per value with the
  * lowest predicted time for UP_CM_ROWS_HINT rows.  Without a model the

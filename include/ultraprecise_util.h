@@ -61,13 +61,26 @@ up_status up_util_compile_only(const up_expr_node* nodes, int32_t n_nodes, int32
 up_status up_util_compile_expr_only(const up_expr_node* nodes, int32_t n_nodes, int32_t root,
                                     const up_col_type* cols, int32_t n_cols, const up_compile_opts* opts);
 
+/* The threads per value an automatic compile would choose (no compile, no
+ * GPU): use_model 0 = the width rule, 1 = the default cost model when one is
+ * set (else the rule). */
+up_status up_util_auto_tpv(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
+                           int32_t n_cols, int32_t use_model, int32_t* threads_per_value);
+
 /* Generated CUDA source of an expression module (no compile, no GPU):
  * returns its length; copies at most cap-1 bytes + NUL when buf != NULL. */
 int64_t up_util_expr_source(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
                             int32_t n_cols, const up_compile_opts* opts, char* buf, int64_t cap);
 
+/* NVRTC-compile a batch module into the cubin cache (no GPU): tpv_of gives
+ * each task's threads per value, NULL the automatic choice (tpv_policy 0). */
 struct up_batch_task;
-up_status up_util_compile_batch_only(const struct up_batch_task* tasks, int32_t n_tasks);
+up_status up_util_compile_batch_only(const struct up_batch_task* tasks, int32_t n_tasks, const int32_t* tpv_of);
+
+/* The threads per value the measured batch policy (tpv_policy 2) times for a
+ * task: writes at most cap of them to out, returns the count (-1: bad
+ * arguments).  One thread per value is always first. */
+int32_t up_util_batch_tpv_candidates(const struct up_batch_task* task, int32_t* out, int32_t cap);
 
 #ifdef __cplusplus
 }

@@ -63,3 +63,23 @@ def test_reference_gradients_match_finite_differences():
         e[i] = h
         num = (ref.loss_and_grads(p + e, X, y)[0] - ref.loss_and_grads(p - e, X, y)[0]) / (2 * h)
         assert abs(num - g[i]) <= 1e-6 + 1e-5 * abs(num), i
+
+
+def test_width_rule_and_batch_candidates():
+    """The automatic threads per value without a model (the width rule) and
+    the group sizes the measured batch policy times."""
+    from ultraprecise_b200 import batch, workloads
+    e, cols = workloads.sweep_expr(600, "mad")
+    assert costmodel.rule_tpv(e, cols) == 16          # 127 limbs: 16 threads of 8 limbs
+    e, cols = workloads.sweep_expr(150, "mad")
+    assert costmodel.rule_tpv(e, cols) == 1           # below the cooperative width
+    e, cols = workloads.sweep_expr(600, "div")
+    assert costmodel.rule_tpv(e, cols) == 1           # divisions: one thread per value
+    a, b = E.col(0), E.col(1)
+    assert costmodel.rule_tpv(a * b, [E.ColType(600, 150, nullable=True), E.ColType(600, 150)]) == 1
+    e, cols = workloads.sweep_expr(600, "mad")
+    cand = batch.tpv_candidates(batch.TaskSpec(e, cols, -1))
+    assert cand[0] == 1 and set(cand[1:]) <= {2, 4, 8, 16, 32} and 16 in cand
+    assert batch.tpv_candidates(batch.TaskSpec(e, cols, 1)) == [1]   # aggregates: one thread
+    e, cols = workloads.sweep_expr(38, "mad")
+    assert batch.tpv_candidates(batch.TaskSpec(e, cols, -1)) == [1]  # narrow: one thread

@@ -190,3 +190,56 @@ def test_rebind_changes_rows():
         assert int(counts.sum()) == rows
         results.append(bytes(o0.cpu().numpy().tobytes()))
     assert results[0] != results[1]
+
+
+def _wide_projections(tasks):
+    """Projection tasks of the bench batch wide enough for cooperative threads."""
+    return [k for k, t in enumerate(tasks) if t["agg"] < 0 and t["p"] > 120]
+
+
+def test_bench_tasks_with_pinned_threads_per_value(bench_batch):
+    """Projection tasks run cooperatively inside the band kernels (and as solo
+    kernels) with every group size: the bytes stay the oracle's."""
+    tasks, data, _, exp, exp_err = bench_batch
+    specs = workloads.batch_specs(tasks)
+    wide = _wide_projections(tasks)
+    assert len(wide) >= 4
+    for kw, sizes in (({}, (4, 8, 16, 32)), ({"solo_rows": 2000}, (8, 16))):
+        b = batch.Batch(specs, tpv_policy=batch.TPV_ONE, **kw)
+        for k, t in enumerate(workloads.batch_pinned_tpv(tasks, sizes)):
+            if t > 1:
+                b.set_task_tpv(k, t)
+        outs, _ = _bind_all(b, tasks, data)
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        b.launch(err)
+        b.launch(err)
+        torch.cuda.synchronize()
+        assert any(b.task_tpv(k) > 1 for k in wide)
+        got = _host(outs, tasks, data, b)
+        for k in range(len(tasks)):
+            assert got[k] == exp[k], f"{kw}: task {k} at {b.task_tpv(k)} threads per value"
+        assert int(err.item()) == exp_err
+
+
+def test_measured_threads_per_value_policy(bench_batch, tmp_path, monkeypatch):
+    """The measured policy times each projection task at its candidate group
+    sizes, keeps one of them, caches the choice, and the bytes stay the
+    oracle's; a second batch reads the cached choices."""
+    monkeypatch.setenv("UP_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
+    tasks, data, _, exp, exp_err = bench_batch
+    specs = workloads.batch_specs(tasks)
+    chosen = []
+    for _ in range(2):
+        b = batch.Batch(specs, tpv_policy=batch.TPV_MEASURED)
+        outs, _ = _bind_all(b, tasks, data)
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        b.launch(err)
+        torch.cuda.synchronize()
+        got = _host(outs, tasks, data, b)
+        for k in range(len(tasks)):
+            assert got[k] == exp[k], f"task {k} at {b.task_tpv(k)} threads per value"
+        assert int(err.item()) == exp_err
+        chosen.append([b.task_tpv(k) for k in range(len(tasks))])
+        assert all(chosen[-1][k] == 1 for k in range(len(tasks)) if tasks[k]["agg"] >= 0)
+    assert chosen[0] == chosen[1]
+    assert "tpv " in (tmp_path / "autotune.txt").read_text()

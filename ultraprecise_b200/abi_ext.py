@@ -24,7 +24,13 @@ SIGNATURES = {
     "up_batch_shape": (_I32, [_P, _I32, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32), C.POINTER(C.c_double)]),
     "up_batch_task_type": (_I32, [_P, _I32, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32)]),
     "up_batch_release": (None, [_P]),
-    "up_util_compile_batch_only": (_I32, [_P, _I32]),
+    "up_util_compile_batch_only": (_I32, [_P, _I32, _P]),
+    "up_batch_task_tpv": (_I32, [_P, _I32, _P]),
+    "up_batch_set_task_tpv": (_I32, [_P, _I32, _I32]),
+    "up_util_batch_tpv_candidates": (_I32, [_P, _P, _I32]),
+    "up_util_auto_tpv": (_I32, [_P, _I32, _I32, _P, _I32, _I32, _P]),
+    "up_costmodel_add_member": (_I32, [_P, _P]),
+    "up_costmodel_set_guard": (_I32, [_P, C.c_float]),
     # ultraprecise_serve.h
     "up_serve_create": (_I32, [_P, C.POINTER(_P)]),
     "up_serve_clock_ms": (C.c_double, [_P]),

@@ -20,7 +20,7 @@ class UpBatchTask(C.Structure):
 
 class UpBatchOpts(C.Structure):
     _fields_ = [("autotune", C.c_int32), ("block_threads", C.c_int32), ("ctas_per_sm", C.c_int32),
-                ("tile_rows", C.c_int32), ("use_graph", C.c_int32), ("reserved", C.c_int32),
+                ("tile_rows", C.c_int32), ("use_graph", C.c_int32), ("tpv_policy", C.c_int32),
                 ("solo_rows", C.c_int64)]
 
 
@@ -48,20 +48,37 @@ def task_array(tasks: Sequence[TaskSpec]):
     return arr, built
 
 
-def compile_only(tasks: Sequence[TaskSpec]) -> None:
-    """NVRTC-compile the batch module into the cubin cache (no GPU needed)."""
+# threads-per-value policies of projection tasks (up_batch_opts.tpv_policy)
+TPV_AUTO, TPV_ONE, TPV_MEASURED = 0, 1, 2
+
+
+def compile_only(tasks: Sequence[TaskSpec], tpv: Sequence[int] | None = None) -> None:
+    """NVRTC-compile the batch module into the cubin cache (no GPU needed);
+    tpv: each task's threads per value (None: the automatic choice)."""
     arr, built = task_array(tasks)
-    abi.check(abi.load().up_util_compile_batch_only(arr, len(tasks)), "up_util_compile_batch_only")
+    tv = None if tpv is None else (C.c_int32 * len(tasks))(*tpv)
+    abi.check(abi.load().up_util_compile_batch_only(arr, len(tasks), tv), "up_util_compile_batch_only")
+
+
+def tpv_candidates(task: TaskSpec):
+    """Threads per value the measured policy times for a task."""
+    arr, built = task_array([task])
+    out = (C.c_int32 * 8)()
+    n = abi.load().up_util_batch_tpv_candidates(arr, out, 8)
+    if n < 0:
+        raise ValueError("bad task")
+    return list(out[:n])
 
 
 class Batch:
     def __init__(self, tasks: Sequence[TaskSpec], autotune: bool = False, use_graph: bool = True,
-                 block_threads: int = 0, ctas_per_sm: int = 0, tile_rows: int = 0, solo_rows: int = 0):
+                 block_threads: int = 0, ctas_per_sm: int = 0, tile_rows: int = 0, solo_rows: int = 0,
+                 tpv_policy: int = TPV_AUTO):
         lib = abi.load()
         self.specs = list(tasks)
         arr, self.built = task_array(tasks)
-        opts = UpBatchOpts(1 if autotune else 0, block_threads, ctas_per_sm, tile_rows, 1 if use_graph else 0, 0,
-                           solo_rows)
+        opts = UpBatchOpts(1 if autotune else 0, block_threads, ctas_per_sm, tile_rows, 1 if use_graph else 0,
+                           tpv_policy, solo_rows)
         h = C.c_void_p()
         abi.check(lib.up_batch_create(arr, len(tasks), C.byref(opts), C.byref(h)), "up_batch_create")
         self._h = h
@@ -88,6 +105,16 @@ class Batch:
         lib = abi.load()
         abi.check(lib.up_batch_launch(self._h, err.data_ptr() if err is not None else None, _stream_ptr(stream)),
                   "up_batch_launch")
+
+    def set_task_tpv(self, k: int, threads_per_value: int) -> None:
+        """Pin task k's threads per value (projection tasks; rebuilt on the next launch)."""
+        abi.check(abi.load().up_batch_set_task_tpv(self._h, k, threads_per_value), "up_batch_set_task_tpv")
+
+    def task_tpv(self, k: int) -> int:
+        """Threads per value task k runs with."""
+        t = C.c_int32()
+        abi.check(abi.load().up_batch_task_tpv(self._h, k, C.byref(t)), "up_batch_task_tpv")
+        return t.value
 
     def shape(self, band: int):
         lib = abi.load()

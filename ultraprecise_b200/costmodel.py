@@ -40,6 +40,18 @@ def features(root: E.Expr, cols: Sequence[E.ColType], tpv: int, rows: int):
     return out, bool(ok.value)
 
 
+def rule_tpv(root: E.Expr, cols: Sequence[E.ColType], use_model: bool = False) -> int:
+    """Threads per value of an automatic compile (no GPU): the width rule, or
+    the default cost model's choice when use_model and one is set."""
+    lib = abi.load()
+    b = E.build([root], cols)
+    E.derive_types(b)
+    t = C.c_int32(1)
+    abi.check(lib.up_util_auto_tpv(b.nodes, b.n_nodes, b.roots[0], b.col_types, b.n_cols, 1 if use_model else 0,
+                                   C.byref(t)), "up_util_auto_tpv")
+    return t.value
+
+
 class CostModel:
     def __init__(self, seed: int = 0):
         lib = abi.load()
@@ -97,6 +109,15 @@ class CostModel:
         abi.check(lib.up_costmodel_choose_tpv(self._h, b.nodes, b.n_nodes, b.roots[0], b.col_types, b.n_cols, rows,
                                               C.byref(t), C.byref(ms)), "up_costmodel_choose_tpv")
         return t.value, float(ms.value)
+
+    def add_member(self, other: "CostModel") -> None:
+        """Average this model's predictions with a copy of `other`'s network."""
+        abi.check(abi.load().up_costmodel_add_member(self._h, other._h), "up_costmodel_add_member")
+
+    def set_guard(self, margin: float) -> None:
+        """Keep the width rule's choice unless at least `margin` of its time
+        is predicted saved."""
+        abi.check(abi.load().up_costmodel_set_guard(self._h, margin), "up_costmodel_set_guard")
 
     def set_default(self) -> None:
         """Make this model the one up_module_compile uses for automatic

@@ -667,6 +667,23 @@ up_status up_util_compile_expr_only(const up_expr_node* nodes, int32_t n_nodes, 
     return jit_compile_cubin(gen.source, cubin);
 }
 
+up_status up_util_auto_tpv(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
+                           int32_t n_cols, int32_t use_model, int32_t* threads_per_value) {
+    if (!nodes || n_nodes <= 0 || !threads_per_value) return fail(UP_ERR_INVALID_ARG, "NULL arguments");
+    std::vector<NodeFacts> f;
+    std::vector<int> topo;
+    up_status st = analyze_nodes(nodes, n_nodes, cols, n_cols, f, topo, {root});
+    if (st != UP_OK) return st;
+    for (int c = 0; c < n_cols; c++)
+        if (cols[c].nullable) {
+            *threads_per_value = 1;
+            return UP_OK;
+        }
+    *threads_per_value = use_model ? auto_threads_per_value(nodes, n_nodes, root, cols, n_cols, f, topo)
+                                   : rule_threads_per_value(nodes, f, topo);
+    return UP_OK;
+}
+
 int64_t up_util_expr_source(const up_expr_node* nodes, int32_t n_nodes, int32_t root, const up_col_type* cols,
                             int32_t n_cols, const up_compile_opts* opts, char* buf, int64_t cap) {
     GeneratedModule gen;

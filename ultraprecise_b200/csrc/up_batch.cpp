@@ -91,6 +91,11 @@ struct up_batch {
     bool prepared = false;
     Shape shape[3];
     bool tuned = false;
+    std::vector<int> tpv;      // threads per value per task (the batch module and the solo modules use it)
+    bool tpv_tuned = false;
+    bool tpv_dirty = false;    // a pinned threads per value is not in the loaded module yet
+    std::vector<bool> tpv_pinned;
+    std::string tpv_key;       // the batch's key before any threads-per-value change (tuning cache)
     cudaGraphExec_t gexec = nullptr;
     uint32_t* graph_err = nullptr;
     cudaStream_t side[2] = {nullptr, nullptr};
@@ -267,8 +272,11 @@ up_status prepare(up_batch* b) {
         up_module* m = nullptr;
         up_status st;
         if (b->t_agg[k] < 0) {
+            up_compile_opts mo;
+            memset(&mo, 0, sizeof mo);
+            mo.threads_per_value = b->tpv[k];
             st = up_module_compile(b->t_nodes[k].data(), (int32_t)b->t_nodes[k].size(), b->t_root[k],
-                                   b->t_cols[k].data(), (int32_t)b->t_cols[k].size(), nullptr, &m);
+                                   b->t_cols[k].data(), (int32_t)b->t_cols[k].size(), &mo, &m);
         } else {
             up_query_agg qa = {b->t_agg[k], b->t_root[k]};
             st = up_query_compile(b->t_nodes[k].data(), (int32_t)b->t_nodes[k].size(), b->t_cols[k].data(),
@@ -414,6 +422,160 @@ up_status autotune(up_batch* b, cudaStream_t s) {
     return UP_OK;
 }
 
+// Threads per value before any measurement: automatic for projections (the
+// default cost model, else the width rule) unless one thread is asked for;
+// aggregates one thread per value.
+std::vector<int> initial_tpv(const up_batch_task* tasks, int n_tasks, int policy) {
+    std::vector<int> tpv(n_tasks, 1);
+    for (int k = 0; k < n_tasks && policy != 1; k++) {
+        if (tasks[k].agg_kind >= 0) continue;
+        std::vector<NodeFacts> f;
+        std::vector<int> topo;
+        if (analyze_nodes(tasks[k].nodes, tasks[k].n_nodes, tasks[k].cols, tasks[k].n_cols, f, topo,
+                          {tasks[k].root}) != UP_OK)
+            continue;  // reported by the module build
+        bool nullable = false;
+        for (int c = 0; c < tasks[k].n_cols; c++) nullable |= tasks[k].cols[c].nullable != 0;
+        if (!nullable)
+            tpv[k] = auto_threads_per_value(tasks[k].nodes, tasks[k].n_nodes, tasks[k].root, tasks[k].cols,
+                                            tasks[k].n_cols, f, topo);
+    }
+    return tpv;
+}
+
+// (Re)generate, compile and load the batch module for the current
+// threads-per-value choices.
+up_status build_module(up_batch* b) {
+    const int n = (int)b->t_nodes.size();
+    std::vector<BatchTaskDesc> desc(n);
+    for (int k = 0; k < n; k++)
+        desc[k] = BatchTaskDesc{b->t_nodes[k].data(), (int)b->t_nodes[k].size(), b->t_root[k], b->t_cols[k].data(),
+                                (int)b->t_cols[k].size(), b->t_agg[k], b->tpv[k]};
+    GeneratedBatch gen;
+    up_status st = generate_batch_module(desc.data(), n, gen);
+    if (st != UP_OK) return st;
+    std::vector<char> cubin;
+    if ((st = jit_compile_linked(gen.units, cubin)) != UP_OK) return st;
+    std::shared_ptr<JitKernelSet> ks;
+    if ((st = jit_load(cubin, gen.kernels, ks)) != UP_OK) return st;
+    b->gen = std::move(gen);
+    b->ks = ks;
+    for (int k = 0; k < n; k++) b->tpv[k] = b->gen.tasks[k].tpv;
+    b->tpv_dirty = false;
+    char key[40];
+    snprintf(key, sizeof key, "%016llx", (unsigned long long)fnv(b->gen.source));
+    b->key = key;
+    return UP_OK;
+}
+
+// Candidate threads per value of a projection task: one thread, and the
+// groups that leave each thread 2..16 limbs of its widest intermediate (a
+// single limb per thread is all shuffles; more than 16 spill).  Tasks narrower
+// than 16 limbs run one thread per value.
+std::vector<int> tpv_candidates(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
+                                int n_cols, int agg) {
+    std::vector<int> c = {1};
+    if (agg >= 0) return c;
+    const int w = coop_width_of(nodes, n_nodes, root, cols, n_cols);
+    if (w < 16) return c;
+    for (int t : {2, 4, 8, 16, 32}) {
+        const int kk = (w + t - 1) / t;
+        if (kk >= 2 && kk <= 16) c.push_back(t);
+    }
+    return c;
+}
+
+// The measured threads-per-value policy: time each projection task's own
+// module at every candidate on its bound inputs (at most 1M rows, into its
+// own output), keep the fastest; the choices are cached with the rows.
+up_status tune_tpv(up_batch* b, cudaStream_t s) {
+    const int n = (int)b->t_nodes.size();
+    std::vector<int> chosen = b->tpv;
+    std::vector<bool> have(n, false);
+    {
+        std::ifstream f(autotune_path());
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream ss(line);
+            std::string tag, key;
+            int task, tpv;
+            long long rows;
+            double ms;
+            if (!(ss >> tag >> key >> task >> rows >> tpv >> ms)) continue;
+            if (tag != "tpv" || key != b->tpv_key || task < 0 || task >= n || b->tpv_pinned[task]) continue;
+            if (rows != (long long)b->host_tasks[task].rows) continue;
+            chosen[task] = tpv;
+            have[task] = true;
+        }
+    }
+    cudaEvent_t e0, e1;
+    UPB_CUDA(cudaEventCreate(&e0));
+    UPB_CUDA(cudaEventCreate(&e1));
+    std::ostringstream lines;
+    up_status st = UP_OK;
+    for (int k = 0; k < n && st == UP_OK; k++) {
+        if (have[k] || b->tpv_pinned[k] || b->t_agg[k] >= 0 || b->host_tasks[k].rows == 0) continue;
+        const std::vector<int> cand = tpv_candidates(b->t_nodes[k].data(), (int)b->t_nodes[k].size(), b->t_root[k],
+                                                     b->t_cols[k].data(), (int)b->t_cols[k].size(), b->t_agg[k]);
+        if (cand.size() < 2) {
+            chosen[k] = 1;
+            continue;
+        }
+        const int64_t rows = std::min<int64_t>(b->host_tasks[k].rows, (int64_t)1 << 20);
+        double best_ms = 1e30;
+        int best = 1;
+        for (int t : cand) {
+            up_compile_opts mo;
+            memset(&mo, 0, sizeof mo);
+            mo.threads_per_value = t;
+            up_module* m = nullptr;
+            if (up_module_compile(b->t_nodes[k].data(), (int32_t)b->t_nodes[k].size(), b->t_root[k],
+                                  b->t_cols[k].data(), (int32_t)b->t_cols[k].size(), &mo, &m) != UP_OK)
+                continue;  // no cooperative form at this width: not a candidate
+            const auto& in = b->t_in[k];
+            double ms_best = 1e30;
+            for (int rep = 0; rep < 3 && st == UP_OK; rep++) {
+                cudaEventRecord(e0, s);
+                st = up_expr_launch(m, in.data(), (int32_t)in.size(), rows, b->host_tasks[k].out, nullptr, s);
+                cudaEventRecord(e1, s);
+                if (cudaEventSynchronize(e1) != cudaSuccess) st = fail(UP_ERR_CUDA, "threads-per-value timing");
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) ms_best = std::min(ms_best, (double)ms);  // the first launch warms up
+            }
+            up_module_release(m);
+            if (ms_best < best_ms) {
+                best_ms = ms_best;
+                best = t;
+            }
+        }
+        chosen[k] = best;
+        lines << "tpv " << b->tpv_key << " " << k << " " << b->host_tasks[k].rows << " " << best << " " << best_ms
+              << "\n";
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != UP_OK) return st;
+    if (!lines.str().empty()) {
+        const std::string p = autotune_path();
+        const std::string dir = p.substr(0, p.rfind('/'));
+        for (size_t i = 1; i <= dir.size(); i++)
+            if (i == dir.size() || dir[i] == '/') mkdir_if_missing(dir.substr(0, i));
+        std::ofstream f(p, std::ios::app);
+        f << lines.str();
+    }
+    b->tpv_tuned = true;
+    if (chosen == b->tpv && !b->tpv_dirty) return UP_OK;
+    b->tpv = chosen;
+    b->drop_device();  // the work lists and the graph belong to the old module
+    for (auto*& m : b->solo_mod)
+        if (m) {
+            up_module_release(m);
+            m = nullptr;
+        }
+    return build_module(b);
+}
+
 }  // namespace
 
 extern "C" {
@@ -421,23 +583,24 @@ extern "C" {
 up_status up_batch_create(const up_batch_task* tasks, int32_t n_tasks, const up_batch_opts* opts, up_batch** out) {
     if (!tasks || !out || n_tasks <= 0) return fail(UP_ERR_INVALID_ARG, "no tasks");
     *out = nullptr;
-    std::vector<BatchTaskDesc> desc(n_tasks);
-    for (int k = 0; k < n_tasks; k++)
-        desc[k] = BatchTaskDesc{tasks[k].nodes, tasks[k].n_nodes, tasks[k].root, tasks[k].cols, tasks[k].n_cols,
-                                tasks[k].agg_kind};
+    if (opts && (opts->tpv_policy < 0 || opts->tpv_policy > 2)) return fail(UP_ERR_INVALID_ARG, "bad tpv_policy");
     auto* b = new up_batch();
-    up_status st = generate_batch_module(desc.data(), n_tasks, b->gen);
-    if (st == UP_OK) {
-        std::vector<char> cubin;
-        st = jit_compile_linked(b->gen.units, cubin);
-        if (st == UP_OK) st = jit_load(cubin, b->gen.kernels, b->ks);
+    if (opts) b->opts = *opts;
+    else b->opts.use_graph = 1;
+    for (int k = 0; k < n_tasks; k++) {
+        b->t_nodes.emplace_back(tasks[k].nodes, tasks[k].nodes + tasks[k].n_nodes);
+        b->t_cols.emplace_back(tasks[k].cols, tasks[k].cols + tasks[k].n_cols);
+        b->t_root.push_back(tasks[k].root);
+        b->t_agg.push_back(tasks[k].agg_kind);
     }
+    b->tpv = initial_tpv(tasks, n_tasks, b->opts.tpv_policy);
+    b->tpv_pinned.assign(n_tasks, false);
+    up_status st = build_module(b);
     if (st != UP_OK) {
         delete b;
         return st;
     }
-    if (opts) b->opts = *opts;
-    else b->opts.use_graph = 1;
+    b->tpv_key = b->key;
     b->host_tasks.assign(n_tasks, HBTask());
     memset(b->host_tasks.data(), 0, sizeof(HBTask) * n_tasks);
     b->bound.assign(n_tasks, false);
@@ -445,12 +608,6 @@ up_status up_batch_create(const up_batch_task* tasks, int32_t n_tasks, const up_
     b->solo.assign(n_tasks, false);
     b->solo_mod.assign(n_tasks, nullptr);
     b->t_in.assign(n_tasks, {});
-    for (int k = 0; k < n_tasks; k++) {
-        b->t_nodes.emplace_back(tasks[k].nodes, tasks[k].nodes + tasks[k].n_nodes);
-        b->t_cols.emplace_back(tasks[k].cols, tasks[k].cols + tasks[k].n_cols);
-        b->t_root.push_back(tasks[k].root);
-        b->t_agg.push_back(tasks[k].agg_kind);
-    }
     for (int k = 0; k < n_tasks; k++) {
         // per-row cost estimate: limb products of every node
         std::vector<NodeFacts> f;
@@ -469,9 +626,6 @@ up_status up_batch_create(const up_batch_task* tasks, int32_t n_tasks, const up_
         s.ctas_per_sm = b->opts.ctas_per_sm > 0 ? b->opts.ctas_per_sm : (band == 2 ? 8 : 4);
         s.tile_rows = b->opts.tile_rows > 0 ? b->opts.tile_rows : (band == 2 ? 256 : 1024);
     }
-    char key[40];
-    snprintf(key, sizeof key, "%016llx", (unsigned long long)fnv(b->gen.source));
-    b->key = key;
     *out = b;
     return UP_OK;
 }
@@ -510,7 +664,21 @@ up_status up_batch_launch(up_batch* b, uint32_t* err_word, void* stream) {
     for (size_t k = 0; k < b->bound.size(); k++)
         if (!b->bound[k]) return fail(UP_ERR_INVALID_ARG, "task " + std::to_string(k) + " is not bound");
     cudaStream_t s = (cudaStream_t)stream;
-    up_status st = prepare(b);
+    up_status st;
+    if (b->opts.tpv_policy == 2 && !b->tpv_tuned) {
+        if ((st = tune_tpv(b, s)) != UP_OK) return st;
+    }
+    if (b->tpv_dirty) {  // pinned threads per value: the module, work lists, solo modules and graph are rebuilt
+        b->drop_device();
+        for (auto*& m : b->solo_mod)
+            if (m) {
+                up_module_release(m);
+                m = nullptr;
+            }
+        if ((st = build_module(b)) != UP_OK) return st;
+    }
+    b->tpv_dirty = false;
+    st = prepare(b);
     if (st != UP_OK) return st;
     if (b->opts.autotune && !b->tuned) {
         if ((st = autotune(b, s)) != UP_OK) return st;
@@ -558,14 +726,45 @@ up_status up_batch_task_type(const up_batch* b, int32_t task, int32_t* precision
     return UP_OK;
 }
 
+up_status up_batch_set_task_tpv(up_batch* b, int32_t task, int32_t threads_per_value) {
+    if (!b || task < 0 || task >= (int)b->tpv.size()) return fail(UP_ERR_INVALID_ARG, "bad task");
+    const int t = threads_per_value;
+    if (t != 1 && t != 2 && t != 4 && t != 8 && t != 16 && t != 32)
+        return fail(UP_ERR_INVALID_ARG, "threads_per_value must be 1, 2, 4, 8, 16 or 32");
+    b->tpv_pinned[task] = true;
+    if (b->tpv[task] != t) {
+        b->tpv[task] = t;
+        b->tpv_dirty = true;
+    }
+    return UP_OK;
+}
+
+up_status up_batch_task_tpv(const up_batch* b, int32_t task, int32_t* threads_per_value) {
+    if (!b || task < 0 || task >= (int)b->tpv.size() || !threads_per_value)
+        return fail(UP_ERR_INVALID_ARG, "bad task");
+    *threads_per_value = b->tpv[task];
+    return UP_OK;
+}
+
 void up_batch_release(up_batch* b) { delete b; }
 
-up_status up_util_compile_batch_only(const up_batch_task* tasks, int32_t n_tasks) {
+int32_t up_util_batch_tpv_candidates(const up_batch_task* task, int32_t* out, int32_t cap) {
+    if (!task || !out || cap <= 0) return -1;
+    const std::vector<int> c =
+        tpv_candidates(task->nodes, task->n_nodes, task->root, task->cols, task->n_cols, task->agg_kind);
+    int n = 0;
+    for (int t : c)
+        if (n < cap) out[n++] = t;
+    return n;
+}
+
+up_status up_util_compile_batch_only(const up_batch_task* tasks, int32_t n_tasks, const int32_t* tpv_of) {
     if (!tasks || n_tasks <= 0) return fail(UP_ERR_INVALID_ARG, "no tasks");
+    const std::vector<int> auto_tpv = initial_tpv(tasks, n_tasks, 0);
     std::vector<BatchTaskDesc> desc(n_tasks);
     for (int k = 0; k < n_tasks; k++)
         desc[k] = BatchTaskDesc{tasks[k].nodes, tasks[k].n_nodes, tasks[k].root, tasks[k].cols, tasks[k].n_cols,
-                                tasks[k].agg_kind};
+                                tasks[k].agg_kind, tpv_of ? tpv_of[k] : auto_tpv[k]};
     GeneratedBatch gen;
     up_status st = generate_batch_module(desc.data(), n_tasks, gen);
     if (st != UP_OK) return st;

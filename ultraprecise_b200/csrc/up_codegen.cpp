@@ -464,6 +464,41 @@ int cooperative_width(const up_expr_node* nodes, const std::vector<NodeFacts>& f
 
 }  // namespace
 
+// The width rule for threads per value (non-nullable inputs): cooperative
+// from kCoopMinLimbs limbs, with the smallest group of at most 8 limbs per
+// thread, except for divisions, which one thread per value runs 2-5x faster
+// on B200 (each long-division step costs a group several broadcasts and
+// ballots).  Automatic threads per value: with a learned cost model set, the
+// model's choice (ultraprecise_costmodel.h), else the rule.  Both return 1
+// for one thread per value.
+int rule_threads_per_value(const up_expr_node* nodes, const std::vector<NodeFacts>& f, const std::vector<int>& topo) {
+    const int w = cooperative_width(nodes, f, topo);
+    if (w <= 0) return 1;
+    bool has_div = false;
+    for (int k : topo)
+        has_div |= nodes[k].kind == UP_NODE_DIV || nodes[k].kind == UP_NODE_MOD ||
+                   (nodes[k].kind == UP_NODE_RESCALE && nodes[k].scale < f[nodes[k].left].scale);
+    if (w < kCoopMinLimbs || has_div) return 1;
+    int t = 2;
+    while (t < 32 && t * 8 < w) t *= 2;
+    return t;
+}
+
+int auto_threads_per_value(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols, int n_cols,
+                           const std::vector<NodeFacts>& f, const std::vector<int>& topo) {
+    if (cooperative_width(nodes, f, topo) <= 0) return 1;
+    const CostChoice cc = default_model_choose_tpv(nodes, n_nodes, root, cols, n_cols);
+    if (cc.valid) return cc.tpv > 1 ? cc.tpv : 1;
+    return rule_threads_per_value(nodes, f, topo);
+}
+
+int coop_width_of(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols, int n_cols) {
+    std::vector<NodeFacts> f;
+    std::vector<int> topo;
+    if (analyze_nodes(nodes, n_nodes, cols, n_cols, f, topo, {root}) != UP_OK) return 0;
+    return cooperative_width(nodes, f, topo);
+}
+
 // ------------------------------------------------- cost-model features
 // Features of launching an expression (ultraprecise_costmodel.h): what the
 // generated kernel's run time depends on — rows, threads per value, limb
@@ -616,34 +651,15 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     {
         const int req = opts ? opts->threads_per_value : 0;
         const int w = cooperative_width(nodes, f, topo);
-        // divisions run cooperatively only on request: measured on B200, one
-        // thread per value divides 2-5x faster (each long-division step costs
-        // the group several broadcasts and ballots)
-        bool has_div = false;
-        for (int k : topo)
-            has_div |= nodes[k].kind == UP_NODE_DIV || nodes[k].kind == UP_NODE_MOD ||
-                       (nodes[k].kind == UP_NODE_RESCALE && nodes[k].scale < f[nodes[k].left].scale);
-        // automatic with a learned cost model set: the threads per value of
-        // the lowest predicted time (ultraprecise_costmodel.h)
-        const CostChoice cc = (req == 0 && w > 0 && !any_nullable)
-                                  ? default_model_choose_tpv(nodes, n_nodes, root, cols, n_cols)
-                                  : CostChoice();
-        if (cc.valid) {
-            if (cc.tpv > 1) {
-                tpiT = cc.tpv;
-                tpiK = (w + tpiT - 1) / tpiT;
-            }
-        } else if (w > 0 && req != 1 && !any_nullable && (req > 1 || (w >= kCoopMinLimbs && !has_div))) {
-            if (req > 1) {
-                tpiT = req;
-            } else {
-                tpiT = 2;
-                while (tpiT < 32 && tpiT * 8 < w) tpiT *= 2;
-            }
-            if (tpiT != 2 && tpiT != 4 && tpiT != 8 && tpiT != 16 && tpiT != 32)
+        if (req > 1 && w > 0 && !any_nullable) {
+            if (req != 2 && req != 4 && req != 8 && req != 16 && req != 32)
                 return fail(UP_ERR_INVALID_ARG, "threads_per_value must be 1, 2, 4, 8, 16 or 32");
-            tpiK = (w + tpiT - 1) / tpiT;
+            tpiT = req;
+        } else if (req == 0 && !any_nullable) {
+            const int t = auto_threads_per_value(nodes, n_nodes, root, cols, n_cols, f, topo);
+            if (t > 1) tpiT = t;
         }
+        if (tpiT > 0) tpiK = (w + tpiT - 1) / tpiT;
     }
     out.threads_per_value = tpiT > 0 ? tpiT : 1;
 
@@ -1464,7 +1480,50 @@ up_status generate_batch_module(const BatchTaskDesc* tasks, int n_tasks, Generat
         for (int n : topo) em.node(n);
         std::ostringstream src;
         src << kBatchPrelude;
-        if (t.agg_kind < 0) {
+        const int wco = cooperative_width(t.nodes, f, topo);
+        gt.tpv = (t.agg_kind < 0 && t.tpv > 1 && wco > 0) ? t.tpv : 1;
+        if (gt.tpv > 1) {
+            // Cooperative projection: groups of T threads per row, K limbs
+            // each; every group of the CTA runs the same number of slots, so
+            // warps stay converged around the shuffles (a group past the last
+            // row works on row r0 and stores nothing).
+            const int TT = gt.tpv, KK = (wco + TT - 1) / TT;
+            if (cmp_root) {
+                gt.out_p = 1;
+                gt.out_s = 0;
+                gt.out_bytes = 1;
+            } else {
+                if (rn.precision < 1) return fail(UP_ERR_INVALID_ARG, "task root precision not set");
+                gt.out_p = rn.precision;
+                gt.out_s = f[t.root].scale;
+                gt.out_bytes = compact_bytes(rn.precision);
+            }
+            const int BO = gt.out_bytes;
+            TEmitter te(t.nodes, t.cols, f, TT, KK);
+            te.plan(topo);
+            for (int n : topo) te.node(n);
+            src << "namespace {\n" << te.globals.str() << "}  // namespace\n";
+            src << "UP_DI u32 trow(" << params_decl(used) << "u8* __restrict__ out, const bool store) {\n";
+            src << "    u32 err = 0u;\n" << te.constants() << te.body.str();
+            if (cmp_root)
+                src << "    if (store && tpi_rank<" << TT << ">() == 0) out[0] = (u8)c" << t.root << ";\n";
+            else
+                src << "    err |= tpi_st<" << TT << ", " << KK << ", " << BO << ">(out, v" << t.root << ", s" << t.root
+                    << ", store);\n";
+            src << "    return err;\n}\n";
+            src << "extern \"C\" __device__ __noinline__ u32 @@tile(const BTask& t, i64 tile, int tr) {\n";
+            src << "    u32 err = 0u;\n    const i64 r0 = tile * tr;\n";
+            src << "    const i64 r1 = (r0 + tr) < t.rows ? (r0 + tr) : t.rows;\n";
+            src << "    const int grp = (int)threadIdx.x / " << TT << ";\n";
+            src << "    const int G = (int)blockDim.x / " << TT << ";\n";
+            src << "    for (i64 base = r0; base < r1; base += G) {\n";
+            src << "        const i64 r = base + grp;\n        const bool valid = r < r1;\n";
+            src << "        const i64 rr = valid ? r : r0;\n";
+            src << "        const u32 e = trow(";
+            for (int c : used) src << "t.col[" << c << "].data + rr * " << gt.in_bytes[c] << ", ";
+            src << "t.out + rr * " << BO << ", valid);\n";
+            src << "        if (valid) err |= e;\n    }\n    return err;\n}\n";
+        } else if (t.agg_kind < 0) {
             if (cmp_root) {
                 gt.out_p = 1;
                 gt.out_s = 0;

@@ -200,10 +200,20 @@ struct up_costmodel {
     float* d_v = nullptr;
     float* d_loss = nullptr;
     cudaStream_t stream = nullptr;
+    // further trained networks whose predictions are averaged with this one's
+    struct Member {
+        std::vector<float> params;
+        float norm[2 * UP_CM_FEATURES + 2];
+        float* d_params = nullptr;
+    };
+    std::vector<Member> members;
+    float guard = 0.0f;  // choose_tpv keeps the width rule unless this fraction of time is predicted saved
     ~up_costmodel() {
         if (stream) cudaStreamSynchronize(stream);
         for (float* p : {d_params, d_m, d_v, d_loss})
             if (p) cudaFree(p);
+        for (auto& mb : members)
+            if (mb.d_params) cudaFree(mb.d_params);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -255,22 +265,43 @@ void standardise(const float* x, int n, const float* norm, float* out) {
         for (int f = 0; f < F; f++) out[(size_t)i * F + f] = (x[(size_t)i * F + f] - norm[f]) / norm[F + f];
 }
 
-up_status predict_locked(up_costmodel* m, const float* feats, int n, float* log_ms) {
-    up_status st = cm_ready(m);
-    if (st != UP_OK) return st;
+// One network's prediction (log ms) with its own parameters and standardisation.
+up_status predict_one(up_costmodel* m, const float* d_params, const float* norm, const float* feats, int n,
+                      float* log_ms) {
     std::vector<float> xs((size_t)n * F);
-    standardise(feats, n, m->norm, xs.data());
+    standardise(feats, n, norm, xs.data());
     DevBuf dx, dout;
     CM_CUDA(cudaMalloc(&dx.p, xs.size() * sizeof(float)));
     CM_CUDA(cudaMalloc(&dout.p, (size_t)n * sizeof(float)));
     CM_CUDA(cudaMemcpyAsync(dx.p, xs.data(), xs.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream));
-    k_mlp_forward<<<(unsigned)((n + 127) / 128), 128, 0, m->stream>>>(m->d_params, (const float*)dx.p, n,
+    k_mlp_forward<<<(unsigned)((n + 127) / 128), 128, 0, m->stream>>>(d_params, (const float*)dx.p, n,
                                                                        (float*)dout.p);
     CM_CUDA(cudaGetLastError());
     std::vector<float> o(n);
     CM_CUDA(cudaMemcpyAsync(o.data(), dout.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
     CM_CUDA(cudaStreamSynchronize(m->stream));
-    for (int i = 0; i < n; i++) log_ms[i] = o[i] * m->norm[2 * F + 1] + m->norm[2 * F];
+    for (int i = 0; i < n; i++) log_ms[i] = o[i] * norm[2 * F + 1] + norm[2 * F];
+    return UP_OK;
+}
+
+// The model's prediction: the mean log ms of its network and its members.
+up_status predict_locked(up_costmodel* m, const float* feats, int n, float* log_ms) {
+    up_status st = cm_ready(m);
+    if (st != UP_OK) return st;
+    if ((st = predict_one(m, m->d_params, m->norm, feats, n, log_ms)) != UP_OK) return st;
+    if (m->members.empty()) return UP_OK;
+    std::vector<double> sum(log_ms, log_ms + n);
+    std::vector<float> one(n);
+    for (auto& mb : m->members) {
+        if (!mb.d_params) {
+            CM_CUDA(cudaMalloc(&mb.d_params, NP * sizeof(float)));
+            CM_CUDA(cudaMemcpyAsync(mb.d_params, mb.params.data(), NP * sizeof(float), cudaMemcpyHostToDevice,
+                                    m->stream));
+        }
+        if ((st = predict_one(m, mb.d_params, mb.norm, feats, n, one.data())) != UP_OK) return st;
+        for (int i = 0; i < n; i++) sum[i] += one[i];
+    }
+    for (int i = 0; i < n; i++) log_ms[i] = (float)(sum[i] / (double)(m->members.size() + 1));
     return UP_OK;
 }
 
@@ -502,8 +533,35 @@ up_status up_costmodel_choose_tpv(up_costmodel* m, const up_expr_node* nodes, in
     int best = 0;
     for (int i = 1; i < nc; i++)
         if (pred[i] < pred[best]) best = i;
+    if (m->guard > 0.0f && nc > 1) {
+        // keep the width rule's choice unless the model predicts it saves at least `guard` of the time
+        std::vector<NodeFacts> f;
+        std::vector<int> topo;
+        if (analyze_nodes(nodes, n_nodes, cols, n_cols, f, topo, {root}) == UP_OK) {
+            const int rt = rule_threads_per_value(nodes, f, topo);
+            for (int i = 0; i < nc; i++)
+                if (cand[i] == rt && pred[best] > pred[i] + std::log(1.0f - m->guard)) best = i;
+        }
+    }
     *tpv = cand[best];
     if (pred_ms) *pred_ms = std::exp(pred[best]);
+    return UP_OK;
+}
+
+up_status up_costmodel_add_member(up_costmodel* m, const up_costmodel* other) {
+    if (!m || !other || m == other) return fail(UP_ERR_INVALID_ARG, "bad models");
+    std::lock_guard<std::mutex> g(m->mu);
+    up_costmodel::Member mb;
+    mb.params = other->params;
+    std::memcpy(mb.norm, other->norm, sizeof mb.norm);
+    m->members.push_back(std::move(mb));
+    return UP_OK;
+}
+
+up_status up_costmodel_set_guard(up_costmodel* m, float margin) {
+    if (!m || !(margin >= 0.0f) || !(margin < 1.0f)) return fail(UP_ERR_INVALID_ARG, "guard must be in [0, 1)");
+    std::lock_guard<std::mutex> g(m->mu);
+    m->guard = margin;
     return UP_OK;
 }
 

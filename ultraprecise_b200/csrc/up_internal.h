@@ -68,6 +68,15 @@ struct CostChoice {
 };
 CostChoice default_model_choose_tpv(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
                                     int n_cols);
+// Automatic threads per value of an expression over non-nullable columns:
+// the default cost model's choice when one is set, else the width rule.
+// Returns 1 for one thread per value.
+int auto_threads_per_value(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols, int n_cols,
+                           const std::vector<NodeFacts>& f, const std::vector<int>& topo);
+// The width rule alone (no cost model).
+int rule_threads_per_value(const up_expr_node* nodes, const std::vector<NodeFacts>& f, const std::vector<int>& topo);
+// Widest limb count of a cooperative evaluation (0: no cooperative form).
+int coop_width_of(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols, int n_cols);
 
 // ------------------------------------------------------------ code generation
 struct GeneratedModule {
@@ -109,6 +118,7 @@ struct BatchTaskDesc {
     const up_col_type* cols;
     int n_cols;
     int agg_kind;  // -1 projection
+    int tpv;       // threads per value of a projection task (1: one thread; 2..32: cooperative)
 };
 struct GeneratedBatch {
     struct Task {
@@ -116,6 +126,7 @@ struct GeneratedBatch {
         int agg = -1;
         int out_p = 0, out_s = 0, out_bytes = 0;
         int nacc = 0, agg_scale = 0;
+        int tpv = 1;  // threads per value the task's tile function runs with
         std::vector<int> in_bytes;
     };
     std::vector<Task> tasks;

@@ -76,9 +76,28 @@ def prewarm(verbose: bool = False) -> None:
             f.result()
             if verbose:
                 print("prewarmed", futs[f])
-    batch.compile_only(workloads.batch_specs(tasks))
+    specs = workloads.batch_specs(tasks)
+    batch.compile_only(specs)
+    batch.compile_only(specs, [1] * len(tasks))  # the one-thread-per-value policy
+    # the pinned cooperative configurations of the GPU tests (at their row cap,
+    # the tasks of at least 2000 rows also run solo)
+    from .expr import ColType  # noqa: F401
+    data_rows = [min(t["rows"], 3001) for t in tasks]
+    for sizes, solo in (((4, 8, 16, 32), False), ((8, 16), True)):
+        tv = workloads.batch_pinned_tpv(tasks, sizes)
+        batch.compile_only(specs, tv)
+        if solo:
+            solo_jobs = [(t["expr"], t["cols"], v) for t, v, r in zip(tasks, tv, data_rows)
+                         if t["agg"] < 0 and r >= 2000]
+            with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+                list(ex.map(lambda j: compile_expr_only(*j), solo_jobs))
+    # every candidate the measured threads-per-value policy times
+    cand_jobs = [(t["expr"], t["cols"], v) for t, spec in zip(tasks, specs)
+                 for v in batch.tpv_candidates(spec) if t["agg"] < 0]
+    with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+        list(ex.map(lambda j: compile_expr_only(*j), cand_jobs))
     if verbose:
-        print("prewarmed batch module,", len(tasks), "tasks")
+        print("prewarmed batch modules,", len(tasks), "tasks,", len(cand_jobs), "threads-per-value candidates")
     # the cooperative-evaluation cases of the GPU tests, with their group sizes
     with cf.ThreadPoolExecutor(max_workers=workers) as ex:
         list(ex.map(lambda c: compile_expr_only(c[2], c[3], c[4]), workloads.coop_cases()))

@@ -326,8 +326,23 @@ def costmodel_train_shapes():
     out = []
     for p in COSTMODEL_TRAIN_P:
         for name, e, n in (("mad", a * b + c, 3), ("mul", a * b, 2), ("div", a / b, 2),
-                           ("sq", (a + b) * (a - b), 2), ("mix", a * b - c * a, 3)):
+                           ("sq", (a + b) * (a - b), 2), ("mix", a * b - c * a, 3),
+                           ("addmul", (a + b) * c, 3), ("divmul", a / b * c, 3), ("twodiv", a / b + c / a, 3)):
             out.append((f"{name} p={p}", e, _cm_cols(p, n)))
+    return out
+
+
+def batch_pinned_tpv(tasks, sizes):
+    """Threads per value pinned on the wide projection tasks (p > 120) of a
+    batch, cycling through `sizes`; 1 elsewhere (the GPU test of cooperative
+    band tasks and its prewarm share it)."""
+    out, i = [], 0
+    for t in tasks:
+        if t["agg"] < 0 and t["p"] > 120:
+            out.append(sizes[i % len(sizes)])
+            i += 1
+        else:
+            out.append(1)
     return out
 
 
