@@ -228,6 +228,60 @@ static long check_div_round(Rng& g, long n, int p, int s) {
     return bad;
 }
 
+// div_small_quotient on x = q*b + r built from a chosen quotient (below 2^48,
+// boundaries included) and remainder (0, 1, b/2 - 1, b/2, b - 1, random).
+template <int NX, int NB>
+static long check_div_small(Rng& g, long n) {
+    long bad = 0, ran = 0;
+    for (long c = 0; c < n; c++) {
+        u32 b[NB];
+        const int len = 2 + g.below(NB - 1);  // wider than one limb
+        gen(g, b, len);
+        uint64_t qq;
+        switch (c % 6) {
+            case 0: qq = (1ull << 48) - 1 - (g.next() % 3); break;
+            case 1: qq = g.next() % 4; break;
+            case 2: qq = 1ull << (g.below(48)); break;
+            default: qq = g.next() & ((1ull << 48) - 1);
+        }
+        // r in [0, b): 0, 1, b - 1, b/2 - 1, b/2 or random below b
+        u32 r[NB], half[NB];
+        for (int i = 0; i < NB; i++) half[i] = (b[i] >> 1) | (i + 1 < NB ? b[i + 1] << 31 : 0u);
+        const int rk = g.below(6);
+        for (int i = 0; i < NB; i++) r[i] = 0u;
+        if (rk == 1) r[0] = 1u;
+        else if (rk == 2) { u32 one[1] = {1u}; sub(r, b, one); }
+        else if (rk == 3) { u32 one[1] = {1u}; sub(r, half, one); }
+        else if (rk == 4) { for (int i = 0; i < NB; i++) r[i] = half[i]; }
+        else if (rk == 5) { gen(g, r, len); if (cmp_n(r, b) >= 0) for (int i = 0; i < NB; i++) r[i] = half[i]; }
+        u32 qv[2] = {(u32)qq, (u32)(qq >> 32)};
+        u32 xw[NX + NB + 2];
+        mul_add(xw, b, qv, r, NB);
+        bool fits = true;
+        for (int i = NX; i < NX + NB + 2; i++) fits &= xw[i] == 0u;
+        if (!fits) continue;  // q*b + r wider than the dividend's static width
+        u32 x[NX];
+        for (int i = 0; i < NX; i++) x[i] = xw[i];
+        // skip inputs the caller would not route here (quotient bound by bit lengths)
+        if (!(bitlen(x) <= bitlen(b) + 47u) || bitlen(b) <= 32u) continue;
+        u32 q[NX];
+        bool up;
+        ran++;
+        div_small_quotient(q, up, x, b);
+        u32 dbl[NB + 1];
+        add(dbl, r, r);
+        const bool want_up = cmp_n(dbl, b) >= 0;
+        bool ok = up == want_up && q[0] == qv[0] && q[1] == qv[1];
+        for (int i = 2; i < NX; i++) ok &= q[i] == 0u;
+        if (!ok) {
+            if (bad < 3) std::printf("div_small<%d,%d> mismatch q=%llu\n", NX, NB, (unsigned long long)qq);
+            bad++;
+        }
+    }
+    std::printf("div_small<%d,%d> %ld %ld\n", NX, NB, ran, bad);
+    return bad + (ran < n / 8 ? 1 : 0);  // the constructed cases must mostly reach the path
+}
+
 int main(int argc, char** argv) {
     const long n = argc > 1 ? std::atol(argv[1]) : 100000;
     Rng g{argc > 2 ? (uint64_t)std::atoll(argv[2]) : 20261203ull};
@@ -244,6 +298,9 @@ int main(int argc, char** argv) {
     bad += check_divmod<41, 32>(g, n / 16);
     bad += check_divmod<24, 5>(g, n / 8);
     bad += check_divmod<72, 63>(g, n / 64);
+    bad += check_div_small<3, 2>(g, n);
+    bad += check_div_small<6, 4>(g, n);
+    bad += check_div_small<8, 4>(g, n);
     bad += check_div_round<2, 1, 8u, 100000000ull>(g, n, 18, 4);
     bad += check_div_round<4, 2, 13u, 10000000000000ull>(g, n, 38, 9);
     bad += check_div_round<8, 3, 23u, 0x2c7e14af6800000ull>(g, n / 2, 76, 19);

@@ -487,6 +487,45 @@ UP_DI void divmod(u32 (&q)[NX], u32 (&rem)[NB], const u32 (&x)[NX], const u32 (&
     shr_bits(rem, rn, s);  // undo the normalising shift
 }
 
+// Quotients below 2^48 of narrow operands (NX + NB <= 12 limbs, divisor
+// wider than one limb, bitlen(x) <= bitlen(b) + 47): q = floor(x / b) from
+// one double division, made exact by one multiply-subtract and at most one
+// correction; up = (2 * (x - q*b) >= b), the half-up decision.  x and b enter
+// as doubles by Horner's rule from the top limb (each of the NX + NB - 2
+// fused steps, the reciprocal and the product round once: relative error
+// below (NX + NB) * 2^-53), so for q < 2^48 the double quotient is within
+// 12/32 of x/b and its floor is q - 1, q or q + 1.
+template <int NX, int NB>
+UP_DI void div_small_quotient(u32 (&q)[NX], bool& up, const u32 (&x)[NX], const u32 (&b)[NB]) {
+    static_assert(NX + NB <= 12, "the error bound needs narrow operands");
+    double X = 0.0, D = 0.0;
+#pragma unroll
+    for (int i = NX - 1; i >= 0; i--) X = __fma_rn(X, 4294967296.0, u32_to_f64(x[i]));
+#pragma unroll
+    for (int i = NB - 1; i >= 0; i--) D = __fma_rn(D, 4294967296.0, u32_to_f64(b[i]));
+    const double Q = __dmul_rn(X, __drcp_rn(D));
+    // floor(Q) (0 <= Q < 2^49) in the low mantissa bits of Q + 2^52 rounded down
+    const double Y = __dadd_rd(Q, 4503599627370496.0);
+    u32 qv[2] = {(u32)__double2loint(Y), (u32)__double2hiint(Y) & 0xfffffu};
+    // r = x - qv * b over NB + 2 limbs, two's complement (|r| < 2b)
+    u32 t[NB + 2], rr[NB + 2];
+    mul(t, b, qv);
+    sub(rr, x, t);
+    if (rr[NB + 1] >> 31) {  // one too large
+        add(rr, rr, b);
+        u32 one[1] = {1u};
+        sub(qv, qv, one);
+    } else if (cmp(rr, b) >= 0) {  // one too small
+        sub(rr, rr, b);
+        add_small(qv, 1u);
+    }
+    u32 dbl[NB + 2];
+    add(dbl, rr, rr);
+    up = cmp(dbl, b) >= 0;
+#pragma unroll
+    for (int i = 0; i < NX; i++) q[i] = i < 2 ? qv[i < 2 ? i : 0] : 0u;
+}
+
 // Bit length of 10^k estimated the way the reference does before choosing
 // the 64-bit divide branch (AriesDecimal.hxx:799-804).
 __host__ __device__ constexpr u32 ref_shift_bits(u32 shift) {
@@ -533,7 +572,11 @@ UP_DI u32 div_round(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32
     mul(x, a, p10);
     u32 q[NX];
     bool up;
-    if (hds <= 32u) {
+    bool small = false;
+    if constexpr (NX + NB <= 12) small = hds > 32u && bitlen(x) <= hds + 47u;
+    if (small) {
+        if constexpr (NX + NB <= 12) div_small_quotient(q, up, x, b);
+    } else if (hds <= 32u) {
         // one-limb divisor: 2/1 steps, whatever NB is; the reference doubles
         // this remainder modulo 2^32
         const u32 b1[1] = {b[0]};
