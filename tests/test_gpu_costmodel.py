@@ -82,9 +82,15 @@ def _eval_times(shape, rows):
 def test_model_beats_or_matches_the_width_rule_on_held_out_shapes():
     X, y, recs, secs = costmodel.collect_samples(workloads.costmodel_train_shapes(), (1 << 18, 1 << 20))
     assert len(y) >= 200
-    m = costmodel.CostModel(seed=3)
-    loss = m.train(X, y, epochs=400, batch=64, lr=3e-3, seed=5)
-    assert loss < 0.2, loss
+    nets = []
+    for k in range(5):  # an ensemble: single networks disagree where the data is thin
+        net = costmodel.CostModel(seed=3 + k)
+        loss = net.train(X, y, epochs=400, batch=64, lr=3e-3, seed=5 + k)
+        assert loss < 0.2, loss
+        nets.append(net)
+    m = nets[0]
+    for net in nets[1:]:
+        m.add_member(net)
     rows = 1 << 20
     tot = {"model": 0.0, "rule": 0.0, "best": 0.0}
     for shape in workloads.costmodel_eval_shapes():
@@ -106,3 +112,19 @@ def test_model_beats_or_matches_the_width_rule_on_held_out_shapes():
         assert runtime.compile_expr(e, cols).threads_per_value == want
     finally:
         costmodel.CostModel.clear_default()
+
+
+def test_ensemble_averages_members_and_guard_keeps_the_rule():
+    rng = np.random.default_rng(5)
+    X = rng.uniform(-1, 1, (64, 16)).astype(np.float32)
+    a, b = costmodel.CostModel(seed=11), costmodel.CostModel(seed=12)
+    ens = costmodel.CostModel(seed=13)
+    ens.set_params(*a.params())
+    ens.add_member(b)
+    np.testing.assert_allclose(ens.predict(X), (a.predict(X) + b.predict(X)) / 2, rtol=1e-5, atol=1e-5)
+    # a guard of 99.9999 %: the width rule's choice unless a 10^6-fold saving is predicted
+    for name, e, cols in workloads.costmodel_eval_shapes():
+        ens.set_guard(0.999999)
+        t, _ = ens.choose_tpv(e, cols, 1 << 20)
+        assert t == costmodel.rule_tpv(e, cols), name
+    ens.set_guard(0.0)

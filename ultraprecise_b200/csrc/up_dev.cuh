@@ -427,14 +427,19 @@ UP_DI void divmod_norm(u32 (&q)[NX], u32 (&rn)[NB], u32 (&bn)[NB], u32& s, const
         u32 w[NB + 1];
 #pragma unroll
         for (int i = 0; i <= NB; i++) w[i] = un[jmax + i];
+        // the next dividend limb is loaded one step ahead (local-memory
+        // latency overlaps the multiply-subtract)
         int j = jmax;
         if constexpr (NB > 40) {
+            u32 nxt = j >= 1 ? un[j - 1] : 0u;
 #pragma unroll 1
             for (; j >= 1; j--) {
+                const u32 cur = nxt;
+                nxt = j >= 2 ? un[j - 2] : 0u;
                 q[j < NX ? j : 0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
                 for (int i = NB; i > 0; i--) w[i] = w[i - 1];
-                w[0] = un[j - 1];
+                w[0] = cur;
             }
             q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
@@ -443,17 +448,19 @@ UP_DI void divmod_norm(u32 (&q)[NX], u32 (&rn)[NB], u32 (&bn)[NB], u32& s, const
         }
 #pragma unroll 1
         for (; j >= 1; j -= 2) {
+            const u32 n1 = un[j - 1];
+            const u32 n2 = j >= 2 ? un[j - 2] : 0u;
             u32 qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
             q[j < NX ? j : 0] = qd;
 #pragma unroll
             for (int i = NB; i > 0; i--) w[i] = w[i - 1];
-            w[0] = un[j - 1];
+            w[0] = n1;
             qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
             q[j - 1] = qd;
             if (j >= 2) {
 #pragma unroll
                 for (int i = NB; i > 0; i--) w[i] = w[i - 1];
-                w[0] = un[j - 2];
+                w[0] = n2;
             }
         }
         if (j == 0) q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
@@ -574,11 +581,18 @@ UP_DI u32 div_round(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32
     bool up;
     bool small = false;
     if constexpr (NX + NB <= 12) small = hds > 32u && bitlen(x) <= hds + 47u;
-    if (small) {
+    if constexpr (NB == 1) {
+        // one-limb divisor: 2/1 steps; the reference doubles this remainder
+        // modulo 2^32 (only this path is compiled: long series inline many
+        // such divisions)
+        u32 r1[1];
+        divmod<NX, 1>(q, r1, x, b);
+        up = (u32)(r1[0] * 2u) >= b[0];
+    } else if (small) {
         if constexpr (NX + NB <= 12) div_small_quotient(q, up, x, b);
     } else if (hds <= 32u) {
-        // one-limb divisor: 2/1 steps, whatever NB is; the reference doubles
-        // this remainder modulo 2^32
+        // a one-limb divisor value: 2/1 steps whatever NB is (the same
+        // doubling modulo 2^32)
         const u32 b1[1] = {b[0]};
         u32 r1[1];
         divmod<NX, 1>(q, r1, x, b1);

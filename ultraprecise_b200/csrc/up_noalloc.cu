@@ -24,17 +24,13 @@
 //     stream) before accumulating; two calls whose work overlaps on the GPU
 //     (different streams, no ordering between them) race on the array and
 //     give wrong results — order them on one stream or with events;
-//   * the first call on a device looks up the array's device address for that
-//     device (cudaGetSymbolAddress, which also loads this library's module on
-//     that device if it is not loaded yet); make that first call before any
-//     stream capture.  The cached address belongs to the device's primary
-//     context, like every module this library loads: a cudaDeviceReset while
-//     the library is in use invalidates both.
+//   * every call looks up the array's device address in the current context
+//     (cudaGetSymbolAddress, which also loads this library's module there the
+//     first time); make the first call on a device before any stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/ultraprecise.h"
@@ -48,33 +44,19 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kMaxDevices];
-
-// Device address of g_noalloc_scratch on the current device, looked up once
-// per device with that device current.  In host code the symbol's name is a
-// host-side stand-in, never a device address.
+// Device address of g_noalloc_scratch in the current context, looked up on
+// every call (cheap), so that a reset device or another context never sees a
+// stale address.  In host code the symbol's name is a host-side stand-in,
+// never a device address.
 up_status noalloc_scratch(void** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
         cudaGetLastError();
-        return fail(UP_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        return fail(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? UP_ERR_NO_DEVICE : UP_ERR_CUDA,
+                    std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
     }
-    if (dev < 0 || dev >= kMaxDevices) return fail(UP_ERR_UNSUPPORTED, "device index above 63");
-    std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return fail(UP_ERR_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") +
-                                         cudaGetErrorString(e));
-        }
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
+    *out = p;
     return UP_OK;
 }
 
