@@ -689,7 +689,9 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
             src << "    err |= tpi_st<" << tpiT << ", " << tpiK << ", " << BO << ">(out, v" << root << ", s" << root
                 << ", store);\n";
         src << "    return err;\n}\n\n";
-        src << "extern \"C\" __global__ void __launch_bounds__(" << CT << ") up_expr_tile(const UpArgs a) {\n";
+        // four CTAs per SM (at most 64 registers): measured on B200, p=600
+        // a*b+c at 16 threads per value 2.27 -> 2.17 ms
+        src << "extern \"C\" __global__ void __launch_bounds__(" << CT << ", 4) up_expr_tile(const UpArgs a) {\n";
         src << "    extern __shared__ __align__(16) u8 sm[];\n";
         src << "    constexpr int R = " << R << ";\n    constexpr int G = " << G << ";\n";
         src << "    const int grp = (int)threadIdx.x / " << tpiT << ";\n";
@@ -813,7 +815,12 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
         }
         const int off_out = smem;
         smem += ((R * BO + 16 + 15) / 16) * 16;
-        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ") up_expr_tile(const UpArgs a) {\n";
+        // The widest rows stage 64 per tile in a 64-thread CTA; asking for six
+        // of them per SM caps registers at 168 (measured on B200: p=300 a*b+c
+        // 1.50 -> 1.40 ms, p=600 a/b 1.24 -> 1.14 ms; with 128-thread CTAs the
+        // same request lets the compiler use more registers and was slower).
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << (T <= 64 ? ", 6" : "")
+            << ") up_expr_tile(const UpArgs a) {\n";
         src << "    extern __shared__ __align__(16) u8 sm[];\n";
         src << "    constexpr int R = " << R << ";\n";
         src << "    const i64 ntiles = (a.rows + R - 1) / R;\n    u32 err = 0u;\n";

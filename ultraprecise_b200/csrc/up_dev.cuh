@@ -384,7 +384,9 @@ UP_DI void divmod_norm(u32 (&q)[NX], u32 (&rn)[NB], u32 (&bn)[NB], u32& s, const
         // copy; a barrel of static shifts would hold several copies of the
         // operands in registers at once.
         const u32 ls = s >> 5, bs = s & 31u;
-        for (int i = 0; i < NU; i++) un[i] = 0u;
+        // zero the limbs the shifted dividend leaves free, below and above it
+        for (int i = 0; i < (int)ls; i++) un[i] = 0u;
+        for (int i = NX + 1 + (int)ls; i < NU; i++) un[i] = 0u;
 #pragma unroll
         for (int i = 0; i <= NX; i++) {
             const u32 hi = i < NX ? x[i < NX ? i : 0] : 0u;
@@ -422,48 +424,25 @@ UP_DI void divmod_norm(u32 (&q)[NX], u32 (&rn)[NB], u32 (&bn)[NB], u32& s, const
         // Wide operands: the rolled loop keeps the current remainder window
         // un[j .. j+NB] in registers (static indices) and moves it down one
         // limb per quotient digit, reading a single dividend limb per step
-        // (up to 40 limbs two digits per iteration, so that half the moves
-        // are renamings; wider windows one digit at a time, for registers).
+        // (one digit per iteration: a two-digit body would save the moves but
+        // double the code of every inlined division of a long expression).
         u32 w[NB + 1];
 #pragma unroll
         for (int i = 0; i <= NB; i++) w[i] = un[jmax + i];
         // the next dividend limb is loaded one step ahead (local-memory
         // latency overlaps the multiply-subtract)
         int j = jmax;
-        if constexpr (NB > 40) {
-            u32 nxt = j >= 1 ? un[j - 1] : 0u;
+        u32 nxt = j >= 1 ? un[j - 1] : 0u;
 #pragma unroll 1
-            for (; j >= 1; j--) {
-                const u32 cur = nxt;
-                nxt = j >= 2 ? un[j - 2] : 0u;
-                q[j < NX ? j : 0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
-#pragma unroll
-                for (int i = NB; i > 0; i--) w[i] = w[i - 1];
-                w[0] = cur;
-            }
-            q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
-#pragma unroll
-            for (int i = 0; i < NB; i++) rn[i] = w[i];
-            return;
-        }
-#pragma unroll 1
-        for (; j >= 1; j -= 2) {
-            const u32 n1 = un[j - 1];
-            const u32 n2 = j >= 2 ? un[j - 2] : 0u;
-            u32 qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
-            q[j < NX ? j : 0] = qd;
+        for (; j >= 1; j--) {
+            const u32 cur = nxt;
+            nxt = j >= 2 ? un[j - 2] : 0u;
+            q[j < NX ? j : 0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
             for (int i = NB; i > 0; i--) w[i] = w[i - 1];
-            w[0] = n1;
-            qd = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
-            q[j - 1] = qd;
-            if (j >= 2) {
-#pragma unroll
-                for (int i = NB; i > 0; i--) w[i] = w[i - 1];
-                w[0] = n2;
-            }
+            w[0] = cur;
         }
-        if (j == 0) q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+        q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
         for (int i = 0; i < NB; i++) rn[i] = w[i];
         return;
@@ -580,7 +559,9 @@ UP_DI u32 div_round(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32
     u32 q[NX];
     bool up;
     bool small = false;
-    if constexpr (NX + NB <= 12) small = hds > 32u && bitlen(x) <= hds + 47u;
+    // (taken where 10^SHIFT leaves at least 16 bits of the 48 for a / b, so
+    // that a warp's rows rarely split between this path and Algorithm D)
+    if constexpr (NX + NB <= 12 && SHIFT <= 9) small = hds > 32u && bitlen(x) <= hds + 47u;
     if constexpr (NB == 1) {
         // one-limb divisor: 2/1 steps; the reference doubles this remainder
         // modulo 2^32 (only this path is compiled: long series inline many
@@ -589,7 +570,7 @@ UP_DI u32 div_round(u32 (&r)[NR], u32& sr, const u32 (&a)[NA], u32 sa, const u32
         divmod<NX, 1>(q, r1, x, b);
         up = (u32)(r1[0] * 2u) >= b[0];
     } else if (small) {
-        if constexpr (NX + NB <= 12) div_small_quotient(q, up, x, b);
+        if constexpr (NX + NB <= 12 && SHIFT <= 9) div_small_quotient(q, up, x, b);
     } else if (hds <= 32u) {
         // a one-limb divisor value: 2/1 steps whatever NB is (the same
         // doubling modulo 2^32)
