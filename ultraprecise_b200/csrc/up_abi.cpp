@@ -79,6 +79,24 @@ int occupancy(void* kernel, int threads, int smem) {
     return n < 1 ? 1 : n;
 }
 
+// Resident CTAs per SM for a tile kernel whose grid loops over tiles: the
+// occupancy limit, lowered for kernels with large per-thread local memory
+// (long expressions of wide values keep many limb arrays there) so that the
+// resident threads' local memory stays within kLocalBytesPerSM: beyond it the
+// arrays fall out of the caches and every access goes to DRAM.
+constexpr int64_t kLocalBytesPerSM = int64_t(4) << 20;
+int resident_ctas(void* kernel, int threads, int smem) {
+    int n = occupancy(kernel, threads, smem);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, (const void*)kernel) != cudaSuccess) {
+        cudaGetLastError();
+        return n;
+    }
+    const int64_t per_cta = (int64_t)fa.localSizeBytes * threads;
+    if (per_cta > 0) n = (int)std::max<int64_t>(1, std::min<int64_t>(n, kLocalBytesPerSM / per_cta));
+    return n;
+}
+
 up_status set_smem(void* kernel, int smem) {
     if (smem > 48 * 1024) {
         UP_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -269,7 +287,8 @@ up_status expr_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64_
         st = set_smem(k, g.smem_bytes);
         if (st != UP_OK) return st;
         const int64_t ntiles = (rows + g.tile_rows - 1) / g.tile_rows;
-        const int64_t cap = spread ? (int64_t)INT32_MAX : (int64_t)sms * occupancy(k, g.block_threads, g.smem_bytes);
+        const int64_t cap =
+            spread ? (int64_t)INT32_MAX : (int64_t)sms * resident_ctas(k, g.block_threads, g.smem_bytes);
         const unsigned grid = (unsigned)std::min<int64_t>(ntiles, cap);
         UP_CUDA(cudaLaunchKernel((const void*)k, dim3(grid), dim3(g.block_threads), args, (size_t)g.smem_bytes, s));
     } else {

@@ -424,25 +424,46 @@ UP_DI void divmod_norm(u32 (&q)[NX], u32 (&rn)[NB], u32 (&bn)[NB], u32& s, const
         // Wide operands: the rolled loop keeps the current remainder window
         // un[j .. j+NB] in registers (static indices) and moves it down one
         // limb per quotient digit, reading a single dividend limb per step
-        // (one digit per iteration: a two-digit body would save the moves but
-        // double the code of every inlined division of a long expression).
+        // (windows above 16 limbs one digit per iteration: measured on B200
+        // the two-digit body, which saves the moves, was slower there and
+        // faster below).
         u32 w[NB + 1];
 #pragma unroll
         for (int i = 0; i <= NB; i++) w[i] = un[jmax + i];
         // the next dividend limb is loaded one step ahead (local-memory
         // latency overlaps the multiply-subtract)
         int j = jmax;
-        u32 nxt = j >= 1 ? un[j - 1] : 0u;
+        if constexpr (NB > 16) {
+            u32 nxt = j >= 1 ? un[j - 1] : 0u;
 #pragma unroll 1
-        for (; j >= 1; j--) {
-            const u32 cur = nxt;
-            nxt = j >= 2 ? un[j - 2] : 0u;
-            q[j < NX ? j : 0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+            for (; j >= 1; j--) {
+                const u32 cur = nxt;
+                nxt = j >= 2 ? un[j - 2] : 0u;
+                q[j < NX ? j : 0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
-            for (int i = NB; i > 0; i--) w[i] = w[i - 1];
-            w[0] = cur;
+                for (int i = NB; i > 0; i--) w[i] = w[i - 1];
+                w[0] = cur;
+            }
+            q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+        } else {
+            // narrow windows: two digits per iteration (half the moves are renamings)
+#pragma unroll 1
+            for (; j >= 1; j -= 2) {
+                const u32 n1 = un[j - 1];
+                const u32 n2 = j >= 2 ? un[j - 2] : 0u;
+                q[j < NX ? j : 0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+#pragma unroll
+                for (int i = NB; i > 0; i--) w[i] = w[i - 1];
+                w[0] = n1;
+                q[j - 1] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
+                if (j >= 2) {
+#pragma unroll
+                    for (int i = NB; i > 0; i--) w[i] = w[i - 1];
+                    w[0] = n2;
+                }
+            }
+            if (j == 0) q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
         }
-        q[0] = knuth_step<NB>(w, bn, est.digit(w[NB], w[NB - 1]));
 #pragma unroll
         for (int i = 0; i < NB; i++) rn[i] = w[i];
         return;
