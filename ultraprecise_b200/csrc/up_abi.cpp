@@ -80,11 +80,16 @@ int occupancy(void* kernel, int threads, int smem) {
 }
 
 // Resident CTAs per SM for a tile kernel whose grid loops over tiles: the
-// occupancy limit, lowered for kernels with large per-thread local memory
-// (long expressions of wide values keep many limb arrays there) so that the
-// resident threads' local memory stays within kLocalBytesPerSM: beyond it the
-// arrays fall out of the caches and every access goes to DRAM.
-constexpr int64_t kLocalBytesPerSM = int64_t(4) << 20;
+// occupancy limit, except for kernels with large per-thread local memory
+// (long expressions of wide values keep many limb arrays there), which keep
+// at most kLocalHeavyThreads threads per SM.  Measured on B200 with the sin
+// series: at p=300 (13 KB of local memory per thread, 128-thread CTAs) two
+// CTAs per SM ran in 27 ms, three (the register limit) in 66 ms and one in
+// 50 ms; at p=1000 (32-thread CTAs) eight CTAs per SM ran in 418 ms and
+// three in 1277 ms.  Kernels with a few KB or less (the divisions) are
+// unaffected.
+constexpr int kLocalHeavyBytes = 4096;
+constexpr int kLocalHeavyThreads = 256;
 int resident_ctas(void* kernel, int threads, int smem) {
     int n = occupancy(kernel, threads, smem);
     cudaFuncAttributes fa;
@@ -92,8 +97,7 @@ int resident_ctas(void* kernel, int threads, int smem) {
         cudaGetLastError();
         return n;
     }
-    const int64_t per_cta = (int64_t)fa.localSizeBytes * threads;
-    if (per_cta > 0) n = (int)std::max<int64_t>(1, std::min<int64_t>(n, kLocalBytesPerSM / per_cta));
+    if (fa.localSizeBytes >= (size_t)kLocalHeavyBytes) n = std::max(1, std::min(n, kLocalHeavyThreads / threads));
     return n;
 }
 
