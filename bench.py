@@ -105,6 +105,12 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: wait (bounded) for its first
+            # line, then keep only the samples taken inside the timed block
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.samples.clear()
         except Exception:
             self.proc = None
         return self
@@ -179,7 +185,7 @@ def build_expr(case):
 # capture, divided by the rows of the captured launch) for the sweep cases
 # profiled so far: profiles/up_expr_tile_p600_mad_cooperative.md,
 # up_expr_tile_p38_mad.md.
-NCU_TRAFFIC_PER_ROW = {(600, "mad"): (196.66e6 + 96.51e6) / 262144, (38, "mad"): 301.58e6 / 4194304}
+NCU_TRAFFIC_PER_ROW = {(600, "mad"): (199.15e6 + 101.88e6) / 262144, (38, "mad"): 301.58e6 / 4194304}
 
 
 # ---------------------------------------------------------- our arm
