@@ -815,11 +815,19 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
         }
         const int off_out = smem;
         smem += ((R * BO + 16 + 15) / 16) * 16;
-        // The widest rows stage 64 per tile in a 64-thread CTA; asking for six
-        // of them per SM caps registers at 168 (measured on B200: p=300 a*b+c
-        // 1.50 -> 1.40 ms, p=600 a/b 1.24 -> 1.14 ms; with 128-thread CTAs the
-        // same request lets the compiler use more registers and was slower).
-        src << "extern \"C\" __global__ void __launch_bounds__(" << T << (T <= 64 ? ", 6" : "")
+        // Minimum resident CTAs per SM, measured on B200.  The widest rows
+        // stage 64 per tile in a 64-thread CTA: six per SM caps registers at
+        // 168 (p=300 a*b+c 1.50 -> 1.40 ms, p=600 a/b 1.24 -> 1.14 ms).
+        // 128-thread CTAs without a division: five per SM, 102 registers
+        // (p=150 a*b+c 0.636 -> 0.547 ms); with divisions the cap spills into
+        // the local memory the digit loop already waits on (p=300 a/b 0.75
+        // -> 0.81 ms), so none is asked for.
+        bool has_div = false;
+        for (int k : topo)
+            has_div |= nodes[k].kind == UP_NODE_DIV || nodes[k].kind == UP_NODE_MOD ||
+                       (nodes[k].kind == UP_NODE_RESCALE && nodes[k].scale < f[nodes[k].left].scale);
+        const char* min_ctas = T <= 64 ? ", 6" : (T == 128 && !has_div ? ", 5" : "");
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << min_ctas
             << ") up_expr_tile(const UpArgs a) {\n";
         src << "    extern __shared__ __align__(16) u8 sm[];\n";
         src << "    constexpr int R = " << R << ";\n";
