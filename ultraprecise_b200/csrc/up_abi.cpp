@@ -480,8 +480,11 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
             // staged tiles; accumulators in registers, shared memory or global
             // memory by group count
             const bool reg = g.q_gr > 0 && n_groups <= g.q_gr;
+            const bool reg_lo = g.q_gr_lo > 0 && n_groups <= g.q_gr_lo;
             const char* reg_name = keys ? "up_query_tile_rk" : "up_query_tile_r";
-            const char* name = reg ? reg_name : (n_groups <= g.q_gs) ? "up_query_tile_s" : "up_query_tile_g";
+            const char* lo_name = keys ? "up_query_tile_rk_lo" : "up_query_tile_r_lo";
+            const char* name = reg_lo ? lo_name : reg ? reg_name : (n_groups <= g.q_gs) ? "up_query_tile_s"
+                                                                                        : "up_query_tile_g";
             a.vec_ok = (vec_ok && keys_aligned) ? 1 : 0;
             const int64_t ntiles = (rows + g.q_tile_rows - 1) / g.q_tile_rows;
             auto launch_tile = [&](const char* kname) -> cudaError_t {
@@ -496,7 +499,8 @@ up_status query_launch_ex(up_module* m, const up_column* in, int32_t n_in, int64
             if (device_count) {
                 // the mode follows the count on the device: every applicable
                 // mode kernel is launched and all but one return at once
-                if (g.q_gr > 0) e = launch_tile(reg_name);
+                if (g.q_gr_lo > 0) e = launch_tile(lo_name);
+                if (e == cudaSuccess && g.q_gr > 0 && n_groups > g.q_gr_lo) e = launch_tile(reg_name);
                 if (e == cudaSuccess && (g.q_gr == 0 || n_groups > g.q_gr)) e = launch_tile("up_query_tile_s");
                 if (e == cudaSuccess && n_groups > g.q_gs) e = launch_tile("up_query_tile_g");
             } else {

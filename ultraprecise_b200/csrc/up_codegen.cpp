@@ -1163,6 +1163,14 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
     for (int n : acc_limbs) reg_words += std::min(n, 4);
     int GR = 0;
     while (GR < 8 && (GR + 1) * reg_words <= 96) GR++;
+    // a second register-mode kernel for fewer groups (the largest power of
+    // two below GR): a row then runs the predicated updates of fewer groups
+    int GRL = 0;
+    if (GR >= 3) {
+        GRL = 1;
+        while (GRL * 2 < GR) GRL *= 2;
+    }
+    out.q_gr_lo = GRL;
     out.q_staged = staged;
     out.q_tile_rows = R;
     out.q_gr = GR;
@@ -1192,9 +1200,11 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         // against the present keys held in registers (the inverse half of the
         // key table), so no table lookup happens per row; rows matching none
         // are counted and flagged as a domain error at the end
-        src << "template <int MODE, int KEYS>\nUP_DI void up_query_tile_body(const UpQArgs& a, u8* sm) {\n";
+        src << "template <int MODE, int KEYS, int GRV>\nUP_DI void up_query_tile_body(const UpQArgs& a, u8* sm) {\n";
         src << "    constexpr int R = " << R << ";\n    constexpr int W = " << W << ";\n";
-        src << "    constexpr int GR = " << std::max(GR, 1) << ";\n";
+        src << "    constexpr int GR = GRV;  // register groups of this kernel\n";
+        // the full register kernel leaves the group counts of the smaller one to it
+        src << "    constexpr int GR_BELOW = GRV == " << std::max(GR, 1) << " ? " << GRL << " : 0;\n";
         src << "    u64* bar = (u64*)(sm + " << off_bar << ");\n";
         src << "    u32* sacc = (u32*)(sm + " << off_acc << ");\n";
         src << "    u32* scnt = (u32*)(sm + " << off_cnt << ");\n";
@@ -1202,8 +1212,8 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         // device every mode is launched and all but one return here
         src << "    const int ng = q_groups(a);\n";
         src << "    if (ng < 0) { if (threadIdx.x == 0 && blockIdx.x == 0 && a.err) atomicOr(a.err, ERR_DOMAIN); return; }\n";
-        src << "    if (MODE == 0 ? ng > " << GR << " : MODE == 1 ? ((" << GR << " > 0 && ng <= " << GR << ") || ng > " << GS
-            << ") : ng <= " << GS << ") return;\n";
+        src << "    if (MODE == 0 ? (ng > GR || ng <= GR_BELOW) : MODE == 1 ? ((" << GR << " > 0 && ng <= " << GR
+            << ") || ng > " << GS << ") : ng <= " << GS << ") return;\n";
         src << "    const int nsm = MODE == 0 ? (ng < GR ? ng : GR) : (MODE == 1 ? ng : 0);\n";
         src << "    for (int i = threadIdx.x; i < nsm * W; i += blockDim.x) sacc[i] = 0u;\n";
         src << "    for (int i = threadIdx.x; i < nsm; i += blockDim.x) scnt[i] = 0u;\n";
@@ -1359,16 +1369,19 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         src << "    err = __reduce_or_sync(0xffffffffu, err);\n";
         src << "    if ((threadIdx.x & 31) == 0 && err != 0u && a.err) atomicOr(a.err, err);\n";
         src << "}\n\n";
-        const char* names[4] = {"up_query_tile_r", "up_query_tile_s", "up_query_tile_g", "up_query_tile_rk"};
-        for (int kn = 0; kn < 4; kn++) {
-            const int mde = kn == 3 ? 0 : kn;
+        const char* names[6] = {"up_query_tile_r",  "up_query_tile_s",    "up_query_tile_g",
+                                "up_query_tile_rk", "up_query_tile_r_lo", "up_query_tile_rk_lo"};
+        for (int kn = 0; kn < 6; kn++) {
+            const int mde = kn == 1 ? 1 : (kn == 2 ? 2 : 0);
+            const int keys = (kn == 3 || kn == 5) ? 1 : 0;
+            const int grv = kn >= 4 ? GRL : std::max(GR, 1);
             if (mde == 0 && GR == 0) continue;
+            if (kn >= 4 && GRL == 0) continue;
             // two CTAs per SM for the register modes (the key-matching one
             // would otherwise take a few registers too many for that)
             src << "extern \"C\" __global__ void __launch_bounds__(" << T << (mde == 0 && T == 256 ? ", 2" : "") << ") "
-                << names[kn]
-                << "(const UpQArgs a) {\n    extern __shared__ __align__(128) u8 sm[];\n    up_query_tile_body<" << mde
-                << ", " << (kn == 3 ? 1 : 0) << ">(a, sm);\n}\n\n";
+                << names[kn] << "(const UpQArgs a) {\n    extern __shared__ __align__(128) u8 sm[];\n"
+                << "    up_query_tile_body<" << mde << ", " << keys << ", " << grv << ">(a, sm);\n}\n\n";
         }
     }
 
@@ -1417,6 +1430,10 @@ up_status generate_query_module(const up_expr_node* nodes, int n_nodes, const up
         if (out.q_gr > 0) {
             out.kernels.push_back("up_query_tile_r");
             out.kernels.push_back("up_query_tile_rk");
+        }
+        if (out.q_gr_lo > 0) {
+            out.kernels.push_back("up_query_tile_r_lo");
+            out.kernels.push_back("up_query_tile_rk_lo");
         }
         out.kernels.push_back("up_query_tile_s");
         out.kernels.push_back("up_query_tile_g");

@@ -96,6 +96,7 @@ struct GeneratedModule {
     bool q_staged = false;        // tile kernels (bulk-copy staged inputs) were generated
     int q_tile_rows = 0;          // rows per tile of the tile kernels
     int q_gr = 0;                 // up_query_tile_r handles n_groups <= q_gr
+    int q_gr_lo = 0;              // up_query_tile_r_lo handles n_groups <= q_gr_lo (0: no such kernel)
     int q_gs = 0;                 // up_query_tile_s handles n_groups <= q_gs
     int q_smem = 0;               // dynamic shared memory of the tile kernels
     long work_per_row = 0;        // limb-product work + bytes per row (scheduling cost estimate)
