@@ -262,6 +262,7 @@ struct TEmitter {
     std::set<int> p10;
     int tmp = 0;
     bool out_of_line = false;  // call multiplies and divisions out of line
+    bool words = false;        // columns come from a padded shared-memory tile (word loads)
 
     TEmitter(const up_expr_node* n, const up_col_type* c, const std::vector<NodeFacts>& facts, int t, int k)
         : nodes(n), cols(c), f(facts), T(t), K(k) {}
@@ -309,7 +310,7 @@ struct TEmitter {
         switch (nd.kind) {
             case UP_NODE_COLUMN: {
                 const int B = compact_bytes(cols[nd.column].precision);
-                body << "    u32 " << v(k) << "[" << K << "]; u32 " << s(k) << "; tpi_ld<" << tk() << ", " << B
+                body << "    u32 " << v(k) << "[" << K << "]; u32 " << s(k) << "; tpi_ld" << (words ? "_words" : "") << "<" << tk() << ", " << B
                      << ">(in" << nd.column << ", " << v(k) << ", " << s(k) << ");\n";
                 break;
             }
@@ -667,6 +668,7 @@ up_status generate_expr_module(const up_expr_node* nodes, int n_nodes, int root,
     int smem = 0;
     if (tpiT > 0) {
         TEmitter te(nodes, cols, f, tpiT, tpiK);
+        te.words = true;  // the columns are read from the staged tile below (padded by 16 bytes)
         te.plan(topo);
         for (int k : topo) te.node(k);
         const int CT = 256;               // CTA threads

@@ -1370,6 +1370,28 @@ UP_DI void tpi_ld(const u8* __restrict__ p, u32 (&x)[K], u32& sign) {
     if (g == TOPL / K) x[TOPL % K] &= CLR;
 }
 
+// tpi_ld from 4-byte-readable memory (a staged shared-memory tile, padded
+// past its last value): one funnel shift of two aligned words per limb
+// instead of four byte loads; the bytes past the value are masked off.
+// Measured on B200: p=600 a*b+c at 16 threads per value 2.18 -> 1.97 ms.
+template <int T, int K, int B>
+UP_DI void tpi_ld_words(const u8* __restrict__ p, u32 (&x)[K], u32& sign) {
+    const int g = tpi_rank<T>();
+    const u32 off = (u32)((unsigned long long)p & 3u);
+    const u32* w = (const u32*)(p - off);
+    const u32 sh = off * 8u;
+    constexpr int W = (B + 3) / 4;  // limbs holding bytes of the value
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        const int L = g * K + i;
+        x[i] = L < W ? __funnelshift_r(w[L], w[L + 1], sh) : 0u;
+    }
+    sign = (u32)(p[B - 1] >> 7);
+    constexpr int TOPL = (B - 1) / 4;
+    constexpr int TOPB = ((B - 1) % 4) * 8 + 7;  // the sign bit; the bits above it belong to the next value
+    if (g == TOPL / K) x[TOPL % K] &= (TOPB == 31) ? 0x7fffffffu : ((1u << TOPB) - 1u);
+}
+
 // This thread's limbs -> bytes [4gK, 4gK+4K) of a B-byte compact value with
 // the sign in bit 7 of byte B-1; ERR_OVERFLOW when a magnitude bit at or
 // above 8*B-1 is set (the same rule as st_compact_bytes).  `store` false
