@@ -110,7 +110,7 @@ def prewarm(verbose: bool = False) -> None:
 
 def prewarm_costmodel(workers: int = 8) -> None:
     """Every cost-model training and held-out shape at every threads per value
-    (the launches the model is trained and judged on)."""
+    (the launches the model is trained and evaluated on)."""
     import concurrent.futures as cf
     shapes = workloads.costmodel_train_shapes() + workloads.costmodel_eval_shapes()
     jobs = [(e, cols, t) for _, e, cols in shapes for t in (1, 2, 4, 8, 16, 32)]
