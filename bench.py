@@ -1139,7 +1139,12 @@ def run_serve(args, rank, world):
                                   f"{args.serve_seconds} s of arrivals each; mix 40/30/20/10 of query/sweep/"
                                   f"batch-task/sin shapes at 1/10 rows; resident columns",
                       "parallelism": f"replicas x{world}", "streams": 8},
-           "rates": rates, "gpu_launches": None, "clocks": clk.summary()}
+           "rates": rates,
+           # at least one launch of a library kernel per served request (a merged
+           # launch serves several), over the sessions
+           "gpu_launches": sum(v[k]["queries"] - v[k].get("merged_requests", 0) + v[k].get("merged_launches", 0)
+                               for v in rates.values() for k in v if isinstance(v[k], dict) and "queries" in v[k]),
+           "clocks": clk.summary()}
     res["roofline"] = None
     return res
 
@@ -1755,7 +1760,10 @@ def run_costmodel(args, rank, world):
             "regret_vs_best": round(tot["model"] / tot["best"], 4),
             "single_network_gain": round(tot["rule"] / tot["single_network"], 4),
             "held_out_log_ms_mae": round(float(np.mean(err)), 4), "shapes": per, "clocks": clk.summary(),
-            "gpu_launches": None}
+            # training steps (one k_mlp_step each), the measured launches of the
+            # samples (a warm-up and three timed each) and of the held-out shapes
+            # (a warm-up and five timed per threads-per-value choice)
+            "gpu_launches": COSTMODEL_ENSEMBLE * 400 * -(-y_n // 64) + 4 * y_n + 6 * len(per) * len(costmodel.TPV_CHOICES)}
 
 
 def runtime_col(rows, p, s, seed):
