@@ -472,6 +472,8 @@ up_status build_module(up_batch* b) {
 // groups that leave each thread 2..16 limbs of its widest intermediate (a
 // single limb per thread is all shuffles; more than 16 spill).  Tasks narrower
 // than 16 limbs run one thread per value.
+constexpr double kTpvMargin = 0.9;  // a cooperative choice must time below 0.9 x one thread per value
+
 std::vector<int> tpv_candidates(const up_expr_node* nodes, int n_nodes, int root, const up_col_type* cols,
                                 int n_cols, int agg) {
     std::vector<int> c = {1};
@@ -522,7 +524,7 @@ up_status tune_tpv(up_batch* b, cudaStream_t s) {
             continue;
         }
         const int64_t rows = std::min<int64_t>(b->host_tasks[k].rows, (int64_t)1 << 20);
-        double best_ms = 1e30;
+        double best_ms = 1e30, one_ms = 1e30;
         int best = 1;
         for (int t : cand) {
             up_compile_opts mo;
@@ -544,10 +546,18 @@ up_status tune_tpv(up_batch* b, cudaStream_t s) {
                 if (rep > 0) ms_best = std::min(ms_best, (double)ms);  // the first launch warms up
             }
             up_module_release(m);
+            if (t == 1) one_ms = ms_best;
             if (ms_best < best_ms) {
                 best_ms = ms_best;
                 best = t;
             }
+        }
+        // a group of threads has to beat one thread per value by kTpvMargin:
+        // timed alone, smaller gains did not survive running beside the other
+        // tasks of the step
+        if (best != 1 && one_ms < 1e30 && best_ms > kTpvMargin * one_ms) {
+            best = 1;
+            best_ms = one_ms;
         }
         chosen[k] = best;
         lines << "tpv " << b->tpv_key << " " << k << " " << b->host_tasks[k].rows << " " << best << " " << best_ms
