@@ -300,9 +300,10 @@ up_status up_query_launch(up_module* m, const up_column* in, int32_t n_in, int64
  * accumulators do not fit (n_groups x accumulator bytes + 8 bytes per group)
  * fail with UP_ERR_INVALID_ARG.  Every GPU that loads the library holds the
  * array until exit; all calls share it, each call clears what it uses on its
- * stream, and calls that overlap on the GPU race.  The first call on a
- * device looks the array up on that device: make it before any stream
- * capture. */
+ * stream, and calls that overlap on the GPU race.  Every call looks the
+ * array's address up in the current context (the first one on a device also
+ * loads the library's module there): make the first call on a device before
+ * any stream capture. */
 up_status up_query_launch_noalloc(up_module* m, const up_column* in, int32_t n_in, int64_t rows,
                                   const int32_t* group_ids, int32_t n_groups,
                                   void* const* outs, uint32_t* err_word, void* stream);
